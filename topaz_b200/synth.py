@@ -1,0 +1,232 @@
+"""Seeded synthetic workloads with the shapes of the TOPAZ benchmark configs.
+
+No public dataset is involved: every residue is drawn from a fixed
+``numpy.random.Generator(PCG64(seed))``.
+
+* Background residues are i.i.d. from the Robinson & Robinson (1991, PNAS
+  88:8880) amino-acid frequencies (the table NCBI BLAST uses).
+* Mutated homologues substitute residue a by b with the BLOSUM62-implied
+  conditional P(b | a, b != a) proportional to q_ab = p_a p_b exp(lambda s_ab),
+  lambda solving sum p_a p_b exp(lambda s_ab) = 1 under those frequencies,
+  and add geometric-length insertions and deletions.
+* Lengths are log-normal with the stated median (sigma 0.6) clipped to the
+  stated range.
+"""
+from __future__ import annotations
+
+import os
+import re
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import alphabet as ab
+
+# Robinson & Robinson background frequencies (per mille), 20 amino acids
+_RR = {
+    "A": 78.05, "C": 19.25, "D": 53.64, "E": 62.95, "F": 38.56, "G": 73.77,
+    "H": 21.99, "I": 51.42, "K": 57.44, "L": 90.19, "M": 22.43, "N": 44.87,
+    "P": 52.03, "Q": 42.64, "R": 51.29, "S": 71.20, "T": 58.41, "V": 64.41,
+    "W": 13.30, "Y": 32.16,
+}
+AA20 = np.frombuffer("".join(sorted(_RR)).encode(), dtype=np.uint8)
+P20 = np.array([_RR[chr(c)] for c in AA20], dtype=np.float64)
+P20 /= P20.sum()
+
+_MATRIX_FILE = os.path.join(os.path.dirname(__file__), "csrc", "tpz_matrices.inc")
+_MATRICES: dict[str, np.ndarray] = {}
+
+
+def matrix(name: str = "BLOSUM62") -> np.ndarray:
+    """25x25 int8 table (row = subject letter, column = query letter) in the
+    order ARNDCQEGHILKMFPSTWYVBJZX*."""
+    if not _MATRICES:
+        text = open(_MATRIX_FILE).read()
+        for blk in re.finditer(r"TPZ_MATRIX_TEXT_(\w+)\[\] =((?:\s*\"[^\"]*\")+);", text):
+            lines = re.findall(r"\"([^\"]*)\"", blk.group(2))
+            rows = [ln.replace("\\n", "").split()[1:] for ln in lines[1:]]
+            _MATRICES[blk.group(1)] = np.array(rows, dtype=np.int8).reshape(25, 25)
+    return _MATRICES[name]
+
+
+def _lambda(m20: np.ndarray, p: np.ndarray) -> float:
+    lo, hi = 1e-3, 2.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        v = (np.outer(p, p) * np.exp(mid * m20)).sum()
+        if v > 1.0:
+            hi = mid
+        else:
+            lo = mid
+    return 0.5 * (lo + hi)
+
+
+_SUB_CACHE = {}
+
+
+def _substitution_table():
+    """Per amino acid a (index into AA20): cumulative P(b | a, b != a)."""
+    if "t" not in _SUB_CACHE:
+        m = matrix("BLOSUM62")
+        idx = ab.aa_to_index(AA20).astype(np.int64)
+        m20 = m[np.ix_(idx, idx)].astype(np.float64)
+        lam = _lambda(m20, P20)
+        q = np.outer(P20, P20) * np.exp(lam * m20)
+        np.fill_diagonal(q, 0.0)
+        q /= q.sum(axis=1, keepdims=True)
+        _SUB_CACHE["t"] = np.cumsum(q, axis=1)
+    return _SUB_CACHE["t"]
+
+
+def lognormal_lengths(rng, n, median, lo, hi, sigma=0.6):
+    x = rng.lognormal(np.log(median), sigma, size=n)
+    return np.clip(np.rint(x), lo, hi).astype(np.int64)
+
+
+def random_residues(rng, n) -> np.ndarray:
+    """n background residues as upper-case amino-acid bytes."""
+    return AA20[rng.choice(20, size=n, p=P20)]
+
+
+def mutate(rng, seq: np.ndarray, identity: float, indel_rate: float = 0.02,
+           indel_p: float = 0.5) -> np.ndarray:
+    """Substitute each residue with probability 1-identity (BLOSUM62
+    conditional), then add insertions/deletions at `indel_rate` per position
+    with geometric(indel_p) lengths."""
+    cum = _substitution_table()
+    pos = np.searchsorted(AA20, seq)
+    out = seq.copy()
+    sub = rng.random(len(seq)) > identity
+    if sub.any():
+        u = rng.random(int(sub.sum()))
+        rows = cum[pos[sub]]
+        out[sub] = AA20[np.minimum((rows < u[:, None]).sum(axis=1), 19)]
+    if indel_rate <= 0:
+        return out
+    pieces = []
+    i = 0
+    n = len(out)
+    events = np.flatnonzero(rng.random(n) < indel_rate)
+    for e in events:
+        if e < i:
+            continue
+        pieces.append(out[i:e])
+        ln = int(rng.geometric(indel_p))
+        if rng.random() < 0.5:
+            pieces.append(random_residues(rng, ln))
+            i = e
+        else:
+            i = e + ln
+    pieces.append(out[i:])
+    return np.concatenate(pieces) if pieces else out
+
+
+# ---------------------------------------------------------------- SW pairs
+
+@dataclass
+class PairSet:
+    """Concatenated query/subject residues (matrix indices) with offsets."""
+    q: np.ndarray       # int8, all queries concatenated
+    qoff: np.ndarray    # int64
+    qlen: np.ndarray    # int32
+    s: np.ndarray       # int8, all subjects concatenated
+    soff: np.ndarray    # int64
+    slen: np.ndarray    # int32
+    seed: int
+
+    @property
+    def n(self):
+        return len(self.qlen)
+
+    @property
+    def cells(self):
+        return int((self.qlen.astype(np.int64) * self.slen.astype(np.int64)).sum())
+
+
+def sw_pairs(n: int, seed: int = 1, q_median=350, q_range=(30, 1000), s_median=350,
+             s_range=(30, 5000), homolog_frac=0.2, identity=(0.25, 0.60)) -> PairSet:
+    """The batched Smith-Waterman microbench workload: n independent pairs,
+    log-normal query/subject lengths, `homolog_frac` of subjects mutated from
+    their query (identity uniform in `identity`, flanked by background to the
+    sampled subject length), the rest background."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    qlen = lognormal_lengths(rng, n, q_median, *q_range)
+    slen = lognormal_lengths(rng, n, s_median, *s_range)
+    hom = rng.random(n) < homolog_frac
+    qtot = int(qlen.sum())
+    q_aa = random_residues(rng, qtot)
+    qoff = np.zeros(n, dtype=np.int64)
+    qoff[1:] = np.cumsum(qlen)[:-1]
+    s_parts = []
+    s_lens = np.empty(n, dtype=np.int64)
+    bg = random_residues(rng, int(slen.sum()))
+    bpos = 0
+    for i in range(n):
+        if hom[i]:
+            core = mutate(rng, q_aa[qoff[i]:qoff[i] + qlen[i]], rng.uniform(*identity))
+            core = core[: s_range[1]]
+            extra = max(0, int(slen[i]) - len(core))
+            left = extra // 2
+            seq = np.concatenate([random_residues(rng, left), core,
+                                  random_residues(rng, extra - left)])
+            if len(seq) < s_range[0]:
+                seq = np.concatenate([seq, random_residues(rng, s_range[0] - len(seq))])
+        else:
+            seq = bg[bpos:bpos + slen[i]]
+            bpos += int(slen[i])
+        s_parts.append(seq)
+        s_lens[i] = len(seq)
+    s_aa = np.concatenate(s_parts)
+    soff = np.zeros(n, dtype=np.int64)
+    soff[1:] = np.cumsum(s_lens)[:-1]
+    return PairSet(ab.aa_to_index(q_aa), qoff, qlen.astype(np.int32),
+                   ab.aa_to_index(s_aa), soff, s_lens.astype(np.int32), seed)
+
+
+# ---------------------------------------------------------- protein DBs
+
+@dataclass
+class Proteins:
+    ids: list
+    seqs: list          # upper-case amino-acid byte arrays
+
+
+def protein_db(n: int, seed: int = 0, median=300, lo=50, hi=2000) -> Proteins:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lens = lognormal_lengths(rng, n, median, lo, hi)
+    allres = random_residues(rng, int(lens.sum()))
+    seqs, off = [], 0
+    for ln in lens:
+        seqs.append(allres[off:off + ln])
+        off += int(ln)
+    return Proteins([f"db{i}" for i in range(n)], seqs)
+
+
+def search_queries(db: Proteins, n_mut: int, n_rand: int, seed: int = 2,
+                   identity=(0.30, 0.70), lo=None, hi=None) -> Proteins:
+    """Queries mutated from randomly chosen DB entries plus random decoys."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ids, seqs = [], []
+    for i in range(n_mut):
+        src = db.seqs[int(rng.integers(len(db.seqs)))]
+        q = mutate(rng, src, rng.uniform(*identity))
+        if lo is not None and len(q) < lo:
+            q = np.concatenate([q, random_residues(rng, lo - len(q))])
+        if hi is not None:
+            q = q[:hi]
+        ids.append(f"mut{i}")
+        seqs.append(q)
+    for i in range(n_rand):
+        ln = int(lognormal_lengths(rng, 1, 300, lo or 50, hi or 2000)[0])
+        ids.append(f"rand{i}")
+        seqs.append(random_residues(rng, ln))
+    return Proteins(ids, seqs)
+
+
+def write_fasta(path: str, prot: Proteins, width: int = 60):
+    with open(path, "wb") as f:
+        for pid, s in zip(prot.ids, prot.seqs):
+            f.write(b">" + pid.encode() + b" synthetic\n")
+            b = s.tobytes()
+            for i in range(0, len(b), width):
+                f.write(b[i:i + width] + b"\n")
