@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the B200 TOPAZ search hot path.
+
+Headline workload (one step): the batched Smith-Waterman microbench --
+1,000,000 (query, subject) pairs, query lengths log-normal (median 350,
+30..1000), subject lengths log-normal (median 350, 30..5000), 80% background
+/ 20% mutated homologues at 25-60% identity, BLOSUM62, gap 11/1, scores and
+end coordinates with the u8 -> i16 -> drop semantics of TOPAZ's ssw_align.
+Seeded synthetic data (no dataset exists for it).  Metric: GCUPS = sum over
+pairs of qlen*slen cells per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
+
+N > 1 runs as torchrun ranks, one GPU each, every rank aligning its own
+1,000,000 pairs (replicas, weak scaling, no data-path collective); the
+timed region is bracketed by barriers and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("queries/s + SW GCUPS at identical hits; batched vs per-pair GPU; p50/p99 ms")
+WORKLOAD = ("batched Smith-Waterman: 1,000,000 pairs/step, qlen lognormal(350) 30-1000, "
+            "slen lognormal(350) 30-5000, 20% homologues 25-60% identity, BLOSUM62 11/1, "
+            "scores+ends (ssw_align u8->i16->drop semantics)")
+DPX_OPS_PER_CELL = 4      # 8 DPX instructions per int16x2 cell pair in the inner loop
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["native", "reference"], default="native")
+    ap.add_argument("--pairs", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of this GPU during the timed region."""
+
+    FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str):
+        self.bus = bus_id.lower()
+        self.rows = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9 and parts[0].lower().endswith(self.bus[-7:]):
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.th:
+            self.th.join(timeout=5)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_baseline_sw(ps, mat, budget_s=12.0):
+    """The reference's own ssw_init+ssw_align (oracle/_ref, compiled from the
+    TOPAZ sources) over all host threads on a bounded sample of the same
+    pairs; falls back to the oracle port when _ref is absent."""
+    import oracle
+    kind = "reference" if oracle.libref() is not None else "port"
+    fn = oracle.reference_sw if kind == "reference" else oracle.oracle_sw
+    threads = os.cpu_count() or 1
+    m = min(ps.n, 4 * threads * 50)
+    t0 = time.perf_counter()
+    fn(ps.q, ps.qoff[:m], ps.qlen[:m], ps.s, ps.soff[:m], ps.slen[:m], mat, 11, 1, threads)
+    dt = time.perf_counter() - t0
+    cells = int((ps.qlen[:m].astype(np.int64) * ps.slen[:m]).sum())
+    if dt < budget_s * 0.5 and m < ps.n:
+        m2 = int(min(ps.n, m * max(1.0, budget_s / max(dt, 1e-3))))
+        t0 = time.perf_counter()
+        fn(ps.q, ps.qoff[:m2], ps.qlen[:m2], ps.s, ps.soff[:m2], ps.slen[:m2], mat, 11, 1, threads)
+        dt = time.perf_counter() - t0
+        m = m2
+        cells = int((ps.qlen[:m].astype(np.int64) * ps.slen[:m]).sum())
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": kind,
+            "sample": "first %d of the %d pairs (%.2f Gcells) in %.1f s" % (m, ps.n, cells / 1e9, dt)}
+
+
+def read_traffic():
+    path = os.path.join(ROOT, "profiles", "sw_microbench_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_cell:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def native_arm(args, rank, local_rank, world):
+    import torch
+    import torch.distributed as dist
+
+    from topaz_b200 import native, synth
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev,
+                                timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ps = synth.sw_pairs(args.pairs, seed=args.seed + 1000 * rank)
+    mat = synth.matrix("BLOSUM62")
+    cells = ps.cells
+    t = {k: torch.from_numpy(np.ascontiguousarray(getattr(ps, k))).to(dev)
+         for k in ("q", "qoff", "qlen", "s", "soff", "slen")}
+    for k in ("score", "ref_end", "read_end", "status"):
+        t[k] = torch.empty(ps.n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # roofline denominator: DPX issue rate on this GPU
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    probe_out = torch.empty(nsm * 8 * 256, dtype=torch.int32, device=dev)
+    for _ in range(2):
+        native.dpx_probe(nsm * 8, 4096, probe_out.data_ptr(), stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ops = native.dpx_probe(nsm * 8, 65536, probe_out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dpx_ops_s = ops / (e0.elapsed_time(e1) / 1e3)
+    peak_gcups = dpx_ops_s / DPX_OPS_PER_CELL / 1e9
+
+    for _ in range(args.warmup):
+        native.sw_batch_torch(t, mat, 11, 1)
+    torch.cuda.synchronize()
+    launches_per_step = native.last_launches()
+    status = t["status"].cpu().numpy()
+    assert (status == native.TPZ_SW_OK).all(), "pairs not aligned: %s" % np.unique(status)
+
+    pr = torch.cuda.get_device_properties(dev)
+    bus = "%08X:%02X:%02X.0" % (getattr(pr, "pci_domain_id", 0), getattr(pr, "pci_bus_id", 0),
+                                getattr(pr, "pci_device_id", 0))
+    clocks = ClockSampler(bus or "")
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for i in range(args.steps):
+        native.sw_batch_torch(t, mat, 11, 1)
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    total_ms = sum(step_ms)
+    tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    max_ms = float(tt.item())
+    value = world * cells * args.steps / (max_ms / 1e3) / 1e9
+    achieved = cells / (total_ms / args.steps / 1e3) / 1e9
+
+    # end to end: host buffers through the C ABI, H2D + D2H inside the step
+    pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(ps, k))).pin_memory()
+           for k in ("q", "qoff", "qlen", "s", "soff", "slen")}
+    outs = {k: torch.empty(ps.n, dtype=torch.int32).pin_memory()
+            for k in ("score", "ref_end", "read_end", "status")}
+    matc = np.ascontiguousarray(mat, dtype=np.int8)
+    L = native.lib()
+
+    def e2e_step():
+        native.check(L.tpz_sw_batch_host(
+            ps.n, pin["q"].data_ptr(), pin["qoff"].data_ptr(), pin["qlen"].data_ptr(),
+            pin["s"].data_ptr(), pin["soff"].data_ptr(), pin["slen"].data_ptr(),
+            matc.ctypes.data, 11, 1, outs["score"].data_ptr(), outs["ref_end"].data_ptr(),
+            outs["read_end"].data_ptr(), outs["status"].data_ptr()))
+
+    e2e_step()
+    assert (outs["score"].numpy() == t["score"].cpu().numpy()).all()
+    barrier()
+    e2e_ms = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        barrier()
+    e2e_val = world * cells * args.steps / float(te.item()) / 1e9
+    h2d = sum(v.numel() * v.element_size() for v in pin.values())
+    d2h = sum(v.numel() * v.element_size() for v in outs.values())
+
+    line = None
+    if rank == 0:
+        cpu = None if args.no_cpu_baseline else cpu_baseline_sw(ps, mat)
+        traffic_per_cell = read_traffic()
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16x2",
+            "data": "synthetic (seeded PCG64; Robinson-Robinson background, BLOSUM62-conditional homologues)",
+            "config": {"workload": WORKLOAD, "pairs_per_step": ps.n, "cells_per_step": cells,
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (%.2f GB resident per step)" % (h2d / 1e9)},
+            "e2e": {"value": round(e2e_val, 2), "unit": "GCUPS", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "step_ms": [round(x, 2) for x in e2e_ms],
+                    "api": "tpz_sw_batch_host (pinned host buffers)"},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "dpx", "achieved": round(achieved, 2),
+                         "peak": round(peak_gcups, 2), "unit": "GCUPS",
+                         "frac": round(achieved / peak_gcups, 4),
+                         "peak_source": "measured live: __viaddmax_s16x2 issue rate %.3e op/s / %d DPX ops per cell"
+                                        % (dpx_ops_s, DPX_OPS_PER_CELL),
+                         "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "step_ms": [round(x, 3) for x in step_ms],
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def reference_arm(args, rank, world):
+    """The reference's own CPU implementation of the path (ssw_init+ssw_align
+    compiled from the TOPAZ sources into oracle/_ref), all host threads, each
+    step a bounded sample of the same workload."""
+    if rank != 0:
+        return None
+    import oracle
+    from topaz_b200 import synth
+    if oracle.libref() is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref (reference build) is not present"}
+    ps = synth.sw_pairs(args.pairs, seed=args.seed)
+    mat = synth.matrix("BLOSUM62")
+    threads = os.cpu_count() or 1
+    # size one step to about 8 s of work
+    m = min(ps.n, 200 * threads)
+    t0 = time.perf_counter()
+    oracle.reference_sw(ps.q, ps.qoff[:m], ps.qlen[:m], ps.s, ps.soff[:m], ps.slen[:m], mat, 11, 1, threads)
+    dt = time.perf_counter() - t0
+    m = int(min(ps.n, max(m, m * 8.0 / max(dt, 1e-3))))
+    times, cells_l = [], []
+    for i in range(args.warmup + args.steps):
+        off = (i * m) % max(1, ps.n - m + 1)
+        sl = slice(off, off + m)
+        t0 = time.perf_counter()
+        oracle.reference_sw(ps.q, ps.qoff[sl], ps.qlen[sl], ps.s, ps.soff[sl], ps.slen[sl], mat, 11, 1, threads)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            cells_l.append(int((ps.qlen[sl].astype(np.int64) * ps.slen[sl]).sum()))
+    value = sum(cells_l) / sum(times) / 1e9
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GCUPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16 SSE2",
+        "data": "synthetic (seeded PCG64)",
+        "config": {"workload": WORKLOAD, "pairs_per_step": m,
+                   "parallelism": "%d host threads" % threads},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads,
+                         "kind": "reference",
+                         "sample": "%d consecutive pairs per step of the 1,000,000-pair workload" % m},
+        "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, local_rank, world = dist_env()
+    if args.warmup < 3 and args.impl == "native":
+        args.warmup = 3
+    if args.impl == "reference":
+        line = reference_arm(args, rank, world)
+    else:
+        line = native_arm(args, rank, local_rank, world)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

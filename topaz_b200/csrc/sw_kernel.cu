@@ -1,0 +1,656 @@
+// sw_kernel.cu -- batched Smith-Waterman (scores + end coordinates) for sm_100a.
+//
+// Result semantics: exactly those of TOPAZ's striped SSW calls
+//   ssw_init(q, qlen, mat, 25, 2); ssw_align(prof, s, slen, go, ge, 0, 0, 0, 15)
+// (src/ssw.c:799-897): the u8 pass, the i16 pass when the u8 pass saturates
+// (max + bias >= 255), and the drop when the i16 pass reaches 32767.
+//
+// The striped u8/i16 passes split the query into 16 (u8) or 8 (i16) SSW
+// "lanes" of seg = ceil(qlen/lanes) consecutive rows.  What they compute is
+// the recurrence below (pinned against src/ssw.c by the oracle tests):
+//   Hp(r,c) = max(0, H(r-1,c-1) + M[s_c][q_r], E(r,c), Fm(r,c))
+//   H(r,c)  = max(Hp(r,c), F(r,c))
+//   E(r,c+1)= max(E(r,c) - ge, Hp(r,c) - go)
+//   Fm(r+1) = (r+1) % seg == 0 ? 0 : max(Fm(r) - ge, Hp(r) - go)
+//   F(r+1)  = max(F(r) - ge, H(r) - go)
+// With X = max(0, H(r-1,c-1) + M, E) and Xg = X - go, and gap_open >
+// gap_extend, this is the same as
+//   H = max(X, F);  Gp = max(Fm - go, Xg);  E' = max(E - ge, Gp)
+//   F' = max(F - ge, Xg);  Fm' = max(Fm - ge, Xg)  (Fm cleared at SSW lane starts)
+// in which the only serial dependences from row to row are the F and Fm
+// chains, one DPX op each.  ref_end is the first column holding the maximum,
+// read_end the smallest row holding it there (src/ssw.c:264-297).
+//
+// Kernel layout (B200): one warp per task of two pairs packed as int16x2
+// (pair A in the low half, pair B in the high half).  Lane t owns query rows
+// [t*R, t*R+R) of both pairs; subject columns stream through the lanes as a
+// wavefront, lane t working on column k-t at step k, with H/F/Fm of a lane's
+// last row and the subject letters handed to lane t+1 by __shfl_up_sync.
+// Every cell update is a DPX instruction (__viaddmax_s16x2[_relu],
+// __vimax_s16x2_relu, __vimax3_s16x2).  The int8 query profile of both pairs
+// sits in shared memory in a lane-blocked layout with an odd word stride per
+// lane, so the 32 per-lane loads of a step never share a bank; prmt with the
+// sign-replicate selector widens two profile bytes into one int16x2 operand.
+//
+// Pairs are binned on the device by R = ceil(qlen/32) and by subject length
+// (counting sort), paired two per task within a bin, and drained by one
+// persistent kernel per R from an atomic task counter.  Pairs whose u8-pass
+// maximum saturates are appended to a rerun list and re-run with the i16
+// lane length (seg = ceil(qlen/8)).  With qlen <= 1024 and |M| <= 127 no
+// score can reach 32767, so 16-bit arithmetic is exact.
+
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "tpz_common.cuh"
+
+namespace tpz {
+namespace sw {
+
+constexpr int kMaxR = 32;           // rows per lane -> qlen <= 1024
+constexpr int kRBins = kMaxR;
+constexpr int kSBins = 256;         // subject-length buckets (32 residues each)
+constexpr int kBins = kRBins * kSBins;
+constexpr int kPadLetter = 25;      // subject column past a pair's end
+constexpr int kPadScore = -64;      // profile value of pad rows / pad columns
+constexpr int kMatStride = 32;      // shared matrix row stride (bytes)
+constexpr int kSmatBytes = 26 * kMatStride;
+
+// bytes per lane block of the profile: 4*W with W odd (bank-conflict free)
+__host__ __device__ constexpr int words_for(int R) {
+    return ((R + 3) / 4) % 2 == 1 ? (R + 3) / 4 : (R + 3) / 4 + 1;
+}
+__host__ __device__ constexpr int profile_bytes(int R) { return 26 * 32 * 4 * words_for(R); }
+__host__ __device__ constexpr int smem_bytes(int R) { return kSmatBytes + 2 * profile_bytes(R); }
+
+struct Args {
+    const int8_t *q;
+    const int64_t *qoff;
+    const int32_t *qlen;
+    const int8_t *s;
+    const int64_t *soff;
+    const int32_t *slen;
+    int32_t *score, *ref_end, *read_end, *status;
+    const int32_t *sorted;   // pair ids sorted by bin
+    const int32_t *rinfo;    // per R bin: [start, count]
+    int32_t *next_task;      // per R bin task counter
+    int32_t *rerun;          // pairs that need the i16 lane length
+    int32_t *rerun_count;
+    int ssw_lanes;           // 16 (u8 pass) or 8 (i16 pass)
+    int gap_open, gap_extend, bias;
+    int8_t mat[625];
+};
+
+__device__ __forceinline__ uint32_t pack2(int lo, int hi) {
+    return (uint32_t)(uint16_t)(int16_t)lo | ((uint32_t)(uint16_t)(int16_t)hi << 16);
+}
+__device__ __forceinline__ int lo16(uint32_t x) { return (int)(int16_t)(x & 0xFFFFu); }
+__device__ __forceinline__ int hi16(uint32_t x) { return (int)(int16_t)(x >> 16); }
+
+__device__ __forceinline__ uint64_t best_key(int v, int col, int row) {
+    return v > 0 ? ((uint64_t)v << 40) | ((uint64_t)(0xFFFFFF - col) << 16) |
+                       (uint64_t)(0xFFFF - row)
+                 : 0ull;
+}
+
+template <int R>
+__device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
+                                         uint32_t *profA, uint32_t *profB) {
+    constexpr int W = words_for(R);
+    const int lane = threadIdx.x & 31;
+    const int i0 = lane * R;
+
+    const int qlA = a.qlen[pA];
+    const int slA = a.slen[pA];
+    const int8_t *qA = a.q + a.qoff[pA];
+    const int8_t *sA = a.s + a.soff[pA];
+    const int qlB = pB >= 0 ? a.qlen[pB] : 0;
+    const int slB = pB >= 0 ? a.slen[pB] : 0;
+    const int8_t *qB = pB >= 0 ? a.q + a.qoff[pB] : qA;
+    const int8_t *sB = pB >= 0 ? a.s + a.soff[pB] : sA;
+    const int N = max(slA, slB);
+
+    // ---- profile of this lane's rows for all 26 letters (25 + pad column)
+    int qa[R], qb[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        qa[r] = (i0 + r < qlA) ? qA[i0 + r] : -1;
+        qb[r] = (i0 + r < qlB) ? qB[i0 + r] : -1;
+    }
+    __syncwarp();
+    for (int let = 0; let < 26; ++let) {
+        const int8_t *mrow = smat + let * kMatStride;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            uint32_t wa = 0, wb = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int r = 4 * w + k;
+                int va = kPadScore, vb = kPadScore;
+                if (r < R) {
+                    if (qa[r] >= 0) va = mrow[qa[r]];
+                    if (qb[r] >= 0) vb = mrow[qb[r]];
+                }
+                wa |= (uint32_t)(uint8_t)(int8_t)va << (8 * k);
+                wb |= (uint32_t)(uint8_t)(int8_t)vb << (8 * k);
+            }
+            profA[(let * 32 + lane) * W + w] = wa;
+            profB[(let * 32 + lane) * W + w] = wb;
+        }
+    }
+    __syncwarp();
+
+    // ---- SSW lane starts of this lane's rows -> per-row clear masks for Fm
+    const int segA = max(1, (qlA + a.ssw_lanes - 1) / a.ssw_lanes);
+    const int segB = max(1, (qlB + a.ssw_lanes - 1) / a.ssw_lanes);
+    uint32_t mask[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        uint32_t m = 0xFFFFFFFFu;
+        if ((i0 + r) % segA == 0) m &= 0xFFFF0000u;
+        if ((i0 + r) % segB == 0) m &= 0x0000FFFFu;
+        mask[r] = m;
+    }
+
+    const uint32_t NGO = pack2(-a.gap_open, -a.gap_open);
+    const uint32_t NGE = pack2(-a.gap_extend, -a.gap_extend);
+    const uint32_t NEGINF = 0x80008000u;
+    // sign-extend byte r%4 of the A word into the low half, of the B word
+    // into the high half
+    constexpr uint32_t SEL[4] = {0xC480u, 0xD591u, 0xE6A2u, 0xF7B3u};
+
+    uint32_t E[R], H[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) { E[r] = 0u; H[r] = 0u; }
+
+    uint32_t outH = 0u, outF = 0u, outFm = 0u, outLet = 0u;
+    uint32_t diag = 0u;
+    uint32_t runmax = 0u;
+    int colA = -1, rowA = 0, colB = -1, rowB = 0;
+
+
+    const int steps = N + 31;
+    for (int k = 0; k < steps; ++k) {
+        uint32_t inH = __shfl_up_sync(0xFFFFFFFFu, outH, 1);
+        uint32_t inF = __shfl_up_sync(0xFFFFFFFFu, outF, 1);
+        uint32_t inFm = __shfl_up_sync(0xFFFFFFFFu, outFm, 1);
+        uint32_t inLet = __shfl_up_sync(0xFFFFFFFFu, outLet, 1);
+        if (lane == 0) {
+            inH = 0u; inF = 0u; inFm = 0u;
+            // the subject letters of column k enter at lane 0 (an L1-resident
+            // byte load; cheaper here than a shuffle-fed prefetch window)
+            const int la = k < slA ? sA[k] : kPadLetter;
+            const int lb = k < slB ? sB[k] : kPadLetter;
+            inLet = (uint32_t)la | ((uint32_t)lb << 8);
+        }
+        const int j = k - lane;
+        if (j >= 0 && j < N) {
+            const uint32_t *pa = profA + ((inLet & 0xFFu) * 32 + lane) * W;
+            const uint32_t *pb = profB + ((inLet >> 8) * 32 + lane) * W;
+            uint32_t wa[W], wb[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) { wa[w] = pa[w]; wb[w] = pb[w]; }
+            uint32_t F = inF, Fm = inFm, D = diag, cm = 0u;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t sc = prmt(wa[r >> 2], wb[r >> 2], SEL[r & 3]);
+                Fm &= mask[r];
+                const uint32_t X = __viaddmax_s16x2_relu(D, sc, E[r]);
+                const uint32_t Hn = __vimax_s16x2_relu(X, F);
+                const uint32_t Xg = __viaddmax_s16x2(X, NGO, NEGINF);
+                const uint32_t Gp = __viaddmax_s16x2(Fm, NGO, Xg);
+                E[r] = __viaddmax_s16x2(E[r], NGE, Gp);
+                F = __viaddmax_s16x2(F, NGE, Xg);
+                Fm = __viaddmax_s16x2(Fm, NGE, Xg);
+                D = H[r];
+                H[r] = Hn;
+                cm = __vimax_s16x2_relu(cm, Hn);
+            }
+            outH = H[R - 1];
+            outF = F;
+            outFm = Fm;
+            outLet = inLet;
+            const uint32_t nm = __vimax_s16x2_relu(runmax, cm);
+            if (nm != runmax) {
+                // the lane's running max rose in this column: remember the
+                // column and the smallest row holding the new value
+                if (lo16(nm) != lo16(runmax)) {
+                    const int v = lo16(nm);
+                    int rr = R;
+#pragma unroll
+                    for (int r = R - 1; r >= 0; --r) if (lo16(H[r]) == v) rr = r;
+                    colA = j; rowA = i0 + rr;
+                }
+                if (hi16(nm) != hi16(runmax)) {
+                    const int v = hi16(nm);
+                    int rr = R;
+#pragma unroll
+                    for (int r = R - 1; r >= 0; --r) if (hi16(H[r]) == v) rr = r;
+                    colB = j; rowB = i0 + rr;
+                }
+                runmax = nm;
+            }
+        }
+        diag = inH;
+    }
+
+    // ---- warp reduction: max value, then first column, then smallest row
+    uint64_t kA = best_key(lo16(runmax), colA, rowA);
+    uint64_t kB = best_key(hi16(runmax), colB, rowB);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kA = max(kA, __shfl_xor_sync(0xFFFFFFFFu, kA, o));
+        kB = max(kB, __shfl_xor_sync(0xFFFFFFFFu, kB, o));
+    }
+    if (lane < 2) {
+        const int p = lane == 0 ? pA : pB;
+        const uint64_t key = lane == 0 ? kA : kB;
+        if (p >= 0) {
+            const int v = (int)(key >> 40);
+            const int col = key ? 0xFFFFFF - (int)((key >> 16) & 0xFFFFFF) : -1;
+            const int row = key ? 0xFFFF - (int)(key & 0xFFFF) : 0;
+            if (a.ssw_lanes == 16 && v + a.bias >= 255) {
+                // u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
+                const int slot = atomicAdd(a.rerun_count, 1);
+                a.rerun[slot] = p;
+            } else {
+                a.score[p] = v;
+                a.ref_end[p] = col;
+                a.read_end[p] = row;
+                a.status[p] = TPZ_SW_OK;
+            }
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    int8_t *smat = reinterpret_cast<int8_t *>(smem);
+    uint32_t *profA = reinterpret_cast<uint32_t *>(smem + kSmatBytes);
+    uint32_t *profB = profA + profile_bytes(R) / 4;
+    const int lane = threadIdx.x;
+    const int bin = R - 1;
+    const int start = a.rinfo[2 * bin];
+    const int count = a.rinfo[2 * bin + 1];
+    const int ntask = (count + 1) / 2;
+    if (ntask == 0) return;
+
+    for (int i = lane; i < 26 * kMatStride; i += 32) {
+        const int r = i / kMatStride, c = i % kMatStride;
+        smat[i] = (r < 25 && c < 25) ? a.mat[r * 25 + c] : (int8_t)kPadScore;
+    }
+    __syncwarp();
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&a.next_task[bin], 1);
+        t = __shfl_sync(0xFFFFFFFFu, t, 0);
+        if (t >= ntask) break;
+        const int pA = a.sorted[start + 2 * t];
+        const int pB = 2 * t + 1 < count ? a.sorted[start + 2 * t + 1] : -1;
+        run_task<R>(a, pA, pB, smat, profA, profB);
+    }
+}
+
+// ---------------------------------------------------------------- binning
+
+__device__ __forceinline__ int pair_bin(int ql, int sl) {
+    const int rb = (ql + 31) / 32 - 1;                  // 0..31
+    const int sb = min(sl >> 5, kSBins - 1);
+    return rb * kSBins + (kSBins - 1 - sb);             // long subjects first
+}
+
+// list == nullptr: pairs 0..n-1; else list[0 .. *list_n)
+__global__ void bin_count_kernel(int64_t n, const int32_t *list, const int32_t *list_n,
+                                 const int32_t *qlen, const int32_t *slen, int32_t *counts,
+                                 int32_t *status) {
+    const int64_t limit = list ? (int64_t)*list_n : n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int p = list ? list[i] : (int)i;
+        const int ql = qlen[p], sl = slen[p];
+        if (ql < 1 || ql > TPZ_SW_MAX_QLEN || sl < 0 || sl >= TPZ_SW_MAX_SLEN) {
+            status[p] = TPZ_SW_INVALID;
+            continue;
+        }
+        atomicAdd(&counts[pair_bin(ql, sl)], 1);
+    }
+}
+
+// one block of 1024 threads: exclusive scan of kBins counts -> cursor; the
+// per-R-bin [start, count] pairs -> rinfo; task counters cleared.
+__global__ void bin_scan_kernel(const int32_t *counts, int32_t *cursor, int32_t *rinfo,
+                                int32_t *next_task) {
+    constexpr int PER = kBins / 1024;
+    __shared__ int32_t part[1024];
+    const int t = threadIdx.x;
+    int32_t loc[PER];
+    int32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) { loc[i] = counts[t * PER + i]; sum += loc[i]; }
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int32_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int32_t run = part[t] - sum;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) { cursor[t * PER + i] = run; run += loc[i]; }
+    __syncthreads();
+    if (t < kRBins) {
+        const int b0 = t * kSBins, b1 = b0 + kSBins;
+        const int32_t s0 = cursor[b0];
+        const int32_t e1 = cursor[b1 - 1] + counts[b1 - 1];
+        rinfo[2 * t] = s0;
+        rinfo[2 * t + 1] = e1 - s0;
+        next_task[t] = 0;
+    }
+}
+
+__global__ void bin_scatter_kernel(int64_t n, const int32_t *list, const int32_t *list_n,
+                                   const int32_t *qlen, const int32_t *slen, int32_t *cursor,
+                                   int32_t *sorted) {
+    const int64_t limit = list ? (int64_t)*list_n : n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int p = list ? list[i] : (int)i;
+        const int ql = qlen[p], sl = slen[p];
+        if (ql < 1 || ql > TPZ_SW_MAX_QLEN || sl < 0 || sl >= TPZ_SW_MAX_SLEN) continue;
+        const int pos = atomicAdd(&cursor[pair_bin(ql, sl)], 1);
+        sorted[pos] = p;
+    }
+}
+
+// ------------------------------------------------------------ roofline probe
+
+// Independent chains of __viaddmax_s16x2 per thread: measures the DPX issue
+// rate the SW kernel is bounded by.  kChains chains per thread, iters steps.
+constexpr int kProbeChains = 8;
+
+__global__ void __launch_bounds__(256) dpx_probe_kernel(int iters, uint32_t inc, uint32_t floor_v,
+                                                        uint32_t *out) {
+    uint32_t acc[kProbeChains];
+#pragma unroll
+    for (int c = 0; c < kProbeChains; ++c) acc[c] = (threadIdx.x + 131u * c) * 0x00010001u;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < kProbeChains; ++c) acc[c] = __viaddmax_s16x2(acc[c], inc, floor_v);
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int c = 0; c < kProbeChains; ++c) x ^= acc[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x;
+}
+
+// ------------------------------------------------------------ host driver
+
+typedef void (*KernelFn)(const Args);
+
+template <int R>
+struct Table {
+    static void fill(KernelFn *k) {
+        k[R - 1] = sw_bin_kernel<R>;
+        Table<R - 1>::fill(k);
+    }
+};
+template <>
+struct Table<0> {
+    static void fill(KernelFn *) {}
+};
+
+constexpr int kAuxStreams = 4;
+
+struct LaunchCfg {
+    KernelFn fn[kMaxR];
+    int smem[kMaxR];
+    int blocks_per_sm[kMaxR];
+    cudaStream_t aux[kAuxStreams];       // bin kernels overlap their tails here
+    cudaEvent_t fork, join[kAuxStreams];
+};
+
+static int launch_cfg(const LaunchCfg **out) {
+    static std::mutex mu;
+    static std::vector<LaunchCfg *> per_dev;
+    int dev = 0;
+    TPZ_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, nullptr);
+    if (!per_dev[dev]) {
+        LaunchCfg *c = new LaunchCfg();
+        Table<kMaxR>::fill(c->fn);
+        for (int r = 1; r <= kMaxR; ++r) {
+            c->smem[r - 1] = smem_bytes(r);
+            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          c->smem[r - 1]));
+            // one carveout for every bin kernel, so blocks of concurrently
+            // running bins can share an SM
+            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
+                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared));
+            int nb = 0;
+            TPZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)c->fn[r - 1],
+                                                                   32, c->smem[r - 1]));
+            c->blocks_per_sm[r - 1] = std::max(1, nb);
+        }
+        for (int i = 0; i < kAuxStreams; ++i) {
+            TPZ_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
+            TPZ_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
+        }
+        TPZ_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+        per_dev[dev] = c;
+    }
+    *out = per_dev[dev];
+    return TPZ_OK;
+}
+
+static thread_local int64_t g_last_launches = 0;
+
+static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t *list,
+                        const int32_t *list_n, int32_t *counts, int32_t *cursor, int32_t *sorted,
+                        cudaStream_t st, int64_t &launches) {
+    const int nsm = sm_count();
+    TPZ_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * kBins, st));
+    const int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
+    bin_count_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, counts,
+                                                      a.status);
+    bin_scan_kernel<<<1, 1024, 0, st>>>(counts, cursor, const_cast<int32_t *>(a.rinfo),
+                                        a.next_task);
+    bin_scatter_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, cursor,
+                                                        sorted);
+    launches += 4;
+    // one persistent kernel per row bin, longest rows first, spread over the
+    // auxiliary streams so that each kernel's tail overlaps the next one
+    TPZ_CUDA(cudaEventRecord(cfg->fork, st));
+    for (int i = 0; i < kAuxStreams; ++i) TPZ_CUDA(cudaStreamWaitEvent(cfg->aux[i], cfg->fork, 0));
+    for (int r = kMaxR; r >= 1; --r) {
+        const int grid = nsm * cfg->blocks_per_sm[r - 1];
+        cudaStream_t xs = cfg->aux[(kMaxR - r) % kAuxStreams];
+        cfg->fn[r - 1]<<<grid, 32, cfg->smem[r - 1], xs>>>(a);
+        ++launches;
+    }
+    for (int i = 0; i < kAuxStreams; ++i) {
+        TPZ_CUDA(cudaEventRecord(cfg->join[i], cfg->aux[i]));
+        TPZ_CUDA(cudaStreamWaitEvent(st, cfg->join[i], 0));
+    }
+    TPZ_CUDA(cudaGetLastError());
+    return TPZ_OK;
+}
+
+int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                 const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
+                 int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
+                 int32_t *status, cudaStream_t st) {
+    g_last_launches = 0;
+    if (n < 0 || n > INT32_MAX / 2 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
+    if (!(go > ge && ge >= 0 && go <= 255)) {
+        set_error("tpz_sw_batch: requires 255 >= gap_open > gap_extend >= 0");
+        return TPZ_E_ARG;
+    }
+    if (n == 0) return TPZ_OK;
+    if (!q || !qoff || !qlen || !s || !soff || !slen || !score || !ref_end || !read_end || !status) {
+        set_error("tpz_sw_batch: NULL buffer");
+        return TPZ_E_ARG;
+    }
+    const LaunchCfg *cfg = nullptr;
+    int rc = launch_cfg(&cfg);
+    if (rc) return rc;
+
+    // workspace: counts, cursor, rinfo, next_task, rerun_count | sorted, rerun
+    const size_t small = sizeof(int32_t) * (2 * kBins + 2 * kRBins + kRBins + 4);
+    const size_t bytes = small + sizeof(int32_t) * 2 * (size_t)n;
+    char *ws = nullptr;
+    TPZ_CUDA(cudaMallocAsync((void **)&ws, bytes, st));
+    int32_t *counts = (int32_t *)ws;
+    int32_t *cursor = counts + kBins;
+    int32_t *rinfo = cursor + kBins;
+    int32_t *next_task = rinfo + 2 * kRBins;
+    int32_t *rerun_count = next_task + kRBins;
+    int32_t *sorted = (int32_t *)(ws + small);
+    int32_t *rerun = sorted + n;
+
+    Args a;
+    a.q = q; a.qoff = qoff; a.qlen = qlen; a.s = s; a.soff = soff; a.slen = slen;
+    a.score = score; a.ref_end = ref_end; a.read_end = read_end; a.status = status;
+    a.sorted = sorted; a.rinfo = rinfo; a.next_task = next_task;
+    a.rerun = rerun; a.rerun_count = rerun_count;
+    a.gap_open = go; a.gap_extend = ge;
+    int mn = 0;
+    for (int i = 0; i < 625; ++i) mn = std::min<int>(mn, mat[i]);
+    a.bias = -mn;
+    memcpy(a.mat, mat, 625);
+
+    int64_t launches = 0;
+    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, sizeof(int32_t), st));
+    a.ssw_lanes = 16;
+    rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, st, launches);
+    if (rc) { cudaFreeAsync(ws, st); return rc; }
+    a.ssw_lanes = 8;
+    rc = launch_round(cfg, a, n, rerun, rerun_count, counts, cursor, sorted, st, launches);
+    if (rc) { cudaFreeAsync(ws, st); return rc; }
+    TPZ_CUDA(cudaFreeAsync(ws, st));
+    g_last_launches = launches;
+    return TPZ_OK;
+}
+
+}  // namespace sw
+}  // namespace tpz
+
+// ------------------------------------------------------------------ C ABI
+
+namespace {
+
+// Grow-only device buffers reused by the host entry point.
+struct HostBatchBuffers {
+    void *p = nullptr;
+    size_t cap = 0;
+    int dev = -1;
+};
+thread_local HostBatchBuffers g_hb;
+thread_local cudaStream_t g_host_stream = nullptr;
+
+int ensure(size_t bytes) {
+    int dev = 0;
+    TPZ_CUDA(cudaGetDevice(&dev));
+    if (g_hb.p && (g_hb.cap >= bytes) && g_hb.dev == dev) return TPZ_OK;
+    if (g_hb.p) cudaFree(g_hb.p);
+    g_hb.p = nullptr;
+    g_hb.cap = 0;
+    TPZ_CUDA(cudaMalloc(&g_hb.p, bytes));
+    g_hb.cap = bytes;
+    g_hb.dev = dev;
+    if (!g_host_stream) TPZ_CUDA(cudaStreamCreateWithFlags(&g_host_stream, cudaStreamNonBlocking));
+    return TPZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpz_sw_batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                        const int8_t *s, const int64_t *soff, const int32_t *slen,
+                        const int8_t *mat625_host, int gap_open, int gap_extend,
+                        int32_t *score, int32_t *ref_end, int32_t *read_end, int32_t *status,
+                        void *stream) {
+    return tpz::sw::batch_device(n, q, qoff, qlen, s, soff, slen, mat625_host, gap_open,
+                                 gap_extend, score, ref_end, read_end, status,
+                                 (cudaStream_t)stream);
+}
+
+int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                      const int8_t *s, const int64_t *soff, const int32_t *slen,
+                      const int8_t *mat625, int gap_open, int gap_extend,
+                      int32_t *score, int32_t *ref_end, int32_t *read_end, int32_t *status) {
+    if (n < 0 || !mat625) { tpz::set_error("tpz_sw_batch_host: n < 0 or NULL matrix"); return TPZ_E_ARG; }
+    if (!(gap_open > gap_extend && gap_extend >= 0 && gap_open <= 255)) {
+        tpz::set_error("tpz_sw_batch_host: requires 255 >= gap_open > gap_extend >= 0");
+        return TPZ_E_ARG;
+    }
+    if (n == 0) return TPZ_OK;
+    // host-side validation: the residue spans must lie inside q / s
+    int64_t qbytes = 0, sbytes = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (qlen[i] < 1 || qlen[i] > TPZ_SW_MAX_QLEN || slen[i] < 0 || slen[i] >= TPZ_SW_MAX_SLEN ||
+            qoff[i] < 0 || soff[i] < 0) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "tpz_sw_batch_host: pair %lld outside the limits (qlen %d, slen %d)",
+                     (long long)i, qlen[i], slen[i]);
+            tpz::set_error(buf);
+            return TPZ_E_RANGE;
+        }
+        qbytes = std::max(qbytes, qoff[i] + qlen[i]);
+        sbytes = std::max(sbytes, soff[i] + slen[i]);
+    }
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t bq = al(qbytes), bs = al(sbytes), b8 = al(8 * (size_t)n), b4 = al(4 * (size_t)n);
+    const size_t total = bq + bs + 2 * b8 + 6 * b4;
+    int rc = ensure(total);
+    if (rc) return rc;
+    char *d = (char *)g_hb.p;
+    int8_t *dq = (int8_t *)d; d += bq;
+    int8_t *ds = (int8_t *)d; d += bs;
+    int64_t *dqoff = (int64_t *)d; d += b8;
+    int64_t *dsoff = (int64_t *)d; d += b8;
+    int32_t *dqlen = (int32_t *)d; d += b4;
+    int32_t *dslen = (int32_t *)d; d += b4;
+    int32_t *dsc = (int32_t *)d; d += b4;
+    int32_t *dre = (int32_t *)d; d += b4;
+    int32_t *drd = (int32_t *)d; d += b4;
+    int32_t *dst = (int32_t *)d; d += b4;
+    cudaStream_t st = g_host_stream;
+    TPZ_CUDA(cudaMemcpyAsync(dq, q, qbytes, cudaMemcpyHostToDevice, st));
+    TPZ_CUDA(cudaMemcpyAsync(ds, s, sbytes, cudaMemcpyHostToDevice, st));
+    TPZ_CUDA(cudaMemcpyAsync(dqoff, qoff, 8 * n, cudaMemcpyHostToDevice, st));
+    TPZ_CUDA(cudaMemcpyAsync(dsoff, soff, 8 * n, cudaMemcpyHostToDevice, st));
+    TPZ_CUDA(cudaMemcpyAsync(dqlen, qlen, 4 * n, cudaMemcpyHostToDevice, st));
+    TPZ_CUDA(cudaMemcpyAsync(dslen, slen, 4 * n, cudaMemcpyHostToDevice, st));
+    rc = tpz::sw::batch_device(n, dq, dqoff, dqlen, ds, dsoff, dslen, mat625, gap_open, gap_extend,
+                               dsc, dre, drd, dst, st);
+    if (rc) return rc;
+    TPZ_CUDA(cudaMemcpyAsync(score, dsc, 4 * n, cudaMemcpyDeviceToHost, st));
+    TPZ_CUDA(cudaMemcpyAsync(ref_end, dre, 4 * n, cudaMemcpyDeviceToHost, st));
+    TPZ_CUDA(cudaMemcpyAsync(read_end, drd, 4 * n, cudaMemcpyDeviceToHost, st));
+    TPZ_CUDA(cudaMemcpyAsync(status, dst, 4 * n, cudaMemcpyDeviceToHost, st));
+    TPZ_CUDA(cudaStreamSynchronize(st));
+    return TPZ_OK;
+}
+
+int64_t tpz_sw_last_launches(void) { return tpz::sw::g_last_launches; }
+
+int tpz_dpx_probe(int64_t blocks, int iters, uint32_t *out, void *stream, int64_t *ops) {
+    if (blocks < 1 || iters < 1 || !out || !ops) { tpz::set_error("tpz_dpx_probe: bad argument"); return TPZ_E_ARG; }
+    tpz::sw::dpx_probe_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(
+        iters, 0x00010001u, 0x80008000u, out);
+    TPZ_CUDA(cudaGetLastError());
+    *ops = blocks * 256 * (int64_t)iters * tpz::sw::kProbeChains;
+    return TPZ_OK;
+}
+
+}  // extern "C"

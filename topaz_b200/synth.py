@@ -83,42 +83,74 @@ def lognormal_lengths(rng, n, median, lo, hi, sigma=0.6):
     return np.clip(np.rint(x), lo, hi).astype(np.int64)
 
 
+# background residues are drawn through a 65536-entry table holding each amino
+# acid round(65536 * p) times (largest-remainder rounding; |error| < 2e-5)
+def _draw_table():
+    raw = P20 * 65536
+    cnt = np.floor(raw).astype(np.int64)
+    rem = raw - cnt
+    cnt[np.argsort(-rem)[: 65536 - cnt.sum()]] += 1
+    return np.repeat(AA20, cnt)
+
+
+_DRAW = _draw_table()
+
+
 def random_residues(rng, n) -> np.ndarray:
     """n background residues as upper-case amino-acid bytes."""
-    return AA20[rng.choice(20, size=n, p=P20)]
+    return _DRAW[rng.integers(0, 65536, size=n, dtype=np.uint16)]
 
 
-def mutate(rng, seq: np.ndarray, identity: float, indel_rate: float = 0.02,
-           indel_p: float = 0.5) -> np.ndarray:
-    """Substitute each residue with probability 1-identity (BLOSUM62
-    conditional), then add insertions/deletions at `indel_rate` per position
-    with geometric(indel_p) lengths."""
+def mutate_batch(rng, seqs: np.ndarray, lens: np.ndarray, identity: np.ndarray,
+                 indel_rate: float = 0.02, indel_p: float = 0.5):
+    """Mutates the concatenated sequences `seqs` (segment lengths `lens`) in
+    one vectorised pass.  Each residue of segment i is substituted with
+    probability 1 - identity[i] (BLOSUM62 conditional); then at rate
+    `indel_rate` per position an insertion (random residues placed before
+    it) or a deletion (of it and the following residues of its segment) of
+    geometric(indel_p) length.  Returns (residues, new segment lengths)."""
+    lens = np.asarray(lens, dtype=np.int64)
+    n = int(lens.sum())
+    seg = np.repeat(np.arange(len(lens)), lens)
+    seg_end = np.cumsum(lens)[seg]
     cum = _substitution_table()
-    pos = np.searchsorted(AA20, seq)
-    out = seq.copy()
-    sub = rng.random(len(seq)) > identity
+    pos = np.searchsorted(AA20, seqs)
+    out = seqs.copy()
+    sub = rng.random(n) > np.asarray(identity, dtype=np.float64)[seg]
     if sub.any():
         u = rng.random(int(sub.sum()))
         rows = cum[pos[sub]]
         out[sub] = AA20[np.minimum((rows < u[:, None]).sum(axis=1), 19)]
-    if indel_rate <= 0:
-        return out
-    pieces = []
-    i = 0
-    n = len(out)
-    events = np.flatnonzero(rng.random(n) < indel_rate)
-    for e in events:
-        if e < i:
-            continue
-        pieces.append(out[i:e])
-        ln = int(rng.geometric(indel_p))
-        if rng.random() < 0.5:
-            pieces.append(random_residues(rng, ln))
-            i = e
-        else:
-            i = e + ln
-    pieces.append(out[i:])
-    return np.concatenate(pieces) if pieces else out
+    if indel_rate <= 0 or n == 0:
+        return out, lens.copy()
+    ev = np.flatnonzero(rng.random(n) < indel_rate)
+    ln = rng.geometric(indel_p, size=len(ev)).astype(np.int64)
+    ins = rng.random(len(ev)) < 0.5
+    # deletions: positions [e, min(e + ln, segment end)) removed
+    diff = np.zeros(n + 1, dtype=np.int64)
+    de, dl = ev[~ins], ln[~ins]
+    np.add.at(diff, de, 1)
+    np.add.at(diff, np.minimum(de + dl, seg_end[de]), -1)
+    keep = np.cumsum(diff[:n]) == 0
+    # insertions: ln random residues before position e
+    ins_len = np.zeros(n, dtype=np.int64)
+    np.add.at(ins_len, ev[ins], ln[ins])
+    counts = ins_len + keep
+    total = int(counts.sum())
+    start = np.cumsum(counts) - counts
+    res = random_residues(rng, total)
+    kp = np.flatnonzero(keep)
+    res[start[kp] + ins_len[kp]] = out[kp]
+    new_lens = np.bincount(seg, weights=counts, minlength=len(lens)).astype(np.int64)
+    return res, new_lens
+
+
+def mutate(rng, seq: np.ndarray, identity: float, indel_rate: float = 0.02,
+           indel_p: float = 0.5) -> np.ndarray:
+    """One sequence through mutate_batch."""
+    out, _ = mutate_batch(rng, seq, np.array([len(seq)]), np.array([identity]), indel_rate,
+                          indel_p)
+    return out
 
 
 # ---------------------------------------------------------------- SW pairs
@@ -143,44 +175,44 @@ class PairSet:
         return int((self.qlen.astype(np.int64) * self.slen.astype(np.int64)).sum())
 
 
+def _segment_positions(starts: np.ndarray, lens: np.ndarray) -> np.ndarray:
+    """Concatenation of arange(starts[i], starts[i] + lens[i])."""
+    lens = np.asarray(lens, dtype=np.int64)
+    total = int(lens.sum())
+    first = np.cumsum(lens) - lens
+    return np.repeat(np.asarray(starts, dtype=np.int64) - first, lens) + np.arange(total)
+
+
 def sw_pairs(n: int, seed: int = 1, q_median=350, q_range=(30, 1000), s_median=350,
              s_range=(30, 5000), homolog_frac=0.2, identity=(0.25, 0.60)) -> PairSet:
     """The batched Smith-Waterman microbench workload: n independent pairs,
     log-normal query/subject lengths, `homolog_frac` of subjects mutated from
-    their query (identity uniform in `identity`, flanked by background to the
-    sampled subject length), the rest background."""
+    their query (identity uniform in `identity`, centred in background
+    residues up to the sampled subject length, cut to the subject range),
+    the rest background."""
     rng = np.random.Generator(np.random.PCG64(seed))
     qlen = lognormal_lengths(rng, n, q_median, *q_range)
     slen = lognormal_lengths(rng, n, s_median, *s_range)
     hom = rng.random(n) < homolog_frac
-    qtot = int(qlen.sum())
-    q_aa = random_residues(rng, qtot)
-    qoff = np.zeros(n, dtype=np.int64)
-    qoff[1:] = np.cumsum(qlen)[:-1]
-    s_parts = []
-    s_lens = np.empty(n, dtype=np.int64)
-    bg = random_residues(rng, int(slen.sum()))
-    bpos = 0
-    for i in range(n):
-        if hom[i]:
-            core = mutate(rng, q_aa[qoff[i]:qoff[i] + qlen[i]], rng.uniform(*identity))
-            core = core[: s_range[1]]
-            extra = max(0, int(slen[i]) - len(core))
-            left = extra // 2
-            seq = np.concatenate([random_residues(rng, left), core,
-                                  random_residues(rng, extra - left)])
-            if len(seq) < s_range[0]:
-                seq = np.concatenate([seq, random_residues(rng, s_range[0] - len(seq))])
-        else:
-            seq = bg[bpos:bpos + slen[i]]
-            bpos += int(slen[i])
-        s_parts.append(seq)
-        s_lens[i] = len(seq)
-    s_aa = np.concatenate(s_parts)
-    soff = np.zeros(n, dtype=np.int64)
-    soff[1:] = np.cumsum(s_lens)[:-1]
-    return PairSet(ab.aa_to_index(q_aa), qoff, qlen.astype(np.int32),
-                   ab.aa_to_index(s_aa), soff, s_lens.astype(np.int32), seed)
+    q_aa = random_residues(rng, int(qlen.sum()))
+    qoff = np.cumsum(qlen) - qlen
+    hid = np.flatnonzero(hom)
+    final_len = slen.copy()
+    if len(hid):
+        core, raw_len = mutate_batch(rng, q_aa[_segment_positions(qoff[hid], qlen[hid])],
+                                     qlen[hid], rng.uniform(*identity, size=len(hid)))
+        raw_off = np.cumsum(raw_len) - raw_len
+        core_len = np.minimum(raw_len, s_range[1])
+        hl = np.maximum(slen[hid], np.maximum(core_len, s_range[0]))
+        final_len[hid] = hl
+    soff = np.cumsum(final_len) - final_len
+    s_aa = random_residues(rng, int(final_len.sum()))
+    if len(hid):
+        left = (hl - core_len) // 2
+        s_aa[_segment_positions(soff[hid] + left, core_len)] = \
+            core[_segment_positions(raw_off, core_len)]
+    return PairSet(ab.aa_to_index(q_aa), qoff.astype(np.int64), qlen.astype(np.int32),
+                   ab.aa_to_index(s_aa), soff.astype(np.int64), final_len.astype(np.int32), seed)
 
 
 # ---------------------------------------------------------- protein DBs
