@@ -41,7 +41,17 @@ enum {
     TPZ_SW_OK = 0,         /* score/ref_end/read_end valid */
     TPZ_SW_DROPPED = 1,    /* 16-bit score reached 32767: ssw_align returns NULL and the
                               hit is dropped (src/ssw.c:866-870, src/ssw_wrapper.c:222-226) */
-    TPZ_SW_INVALID = 2     /* pair outside the stated limits; not aligned */
+    TPZ_SW_INVALID = 2,    /* pair outside the stated limits; not aligned */
+    TPZ_SW_GAPLESS_LOW = 3 /* search hit with gapless score < 40: no SW, bitscore 0,
+                              E-value 1000 (src/ssw_wrapper.c:171-176) */
+};
+
+/* Per-query status bits of tpz_search_batch. */
+enum {
+    TPZ_Q_SA_END = 1,      /* the walk reached a suffix-array row past the zero-filled
+                              last page of the .SA mapping, where the reference reads
+                              unmapped memory; the query stopped there */
+    TPZ_Q_TOO_LONG = 2     /* query longer than TPZ_SEARCH_MAX_QLEN: not searched */
 };
 
 TPZ_API const char *tpz_last_error(void);
@@ -84,6 +94,83 @@ TPZ_API int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, c
 /* Kernel launches enqueued by the last tpz_sw_batch_* call on this thread
  * (for launch accounting). */
 TPZ_API int64_t tpz_sw_last_launches(void);
+
+/* ------------------------------------------------------------------------
+ * Resident index: the .psq text, .SA and .ind of one database copied into
+ * device memory once (db_load, src/db.c:34-126) plus derived tables.
+ * T: Tsize bytes (internal alphabet, '\n' after every protein); SA: Tsize
+ * int64; ind: Psize packed 24-byte records {u64 header_start, u64
+ * protein_start, i32 header_len, i32 protein_len} (src/db.h:10-17).
+ * Returns TPZ_E_ARG when the three do not describe one database.
+ * ------------------------------------------------------------------------ */
+typedef struct tpz_index tpz_index;
+
+TPZ_API int tpz_index_create(const uint8_t *T, int64_t Tsize, const int64_t *SA, const void *ind,
+                             int64_t Psize, tpz_index **out);
+TPZ_API void tpz_index_destroy(tpz_index *ix);
+TPZ_API int64_t tpz_index_device_bytes(const tpz_index *ix);
+
+/* sa_search (src/search.c:237-362, declared src/search.h:14) for n whole
+ * patterns pcat[poff[i] .. +plen[i]) (internal alphabet letters, plen >= 1):
+ * idx[i] = the lower bound = number of suffixes smaller than the pattern. */
+TPZ_API int tpz_sa_search_batch(const tpz_index *ix, const char *pcat, const int64_t *poff,
+                                const int32_t *plen, int64_t n, int64_t *idx);
+
+/* sa_hsp (src/search.c:99-190, declared src/search.h:13) for n (query,
+ * offset, SA row) triples: score/length of the two-sided gapless extension;
+ * length -1 when the first symbols differ (score then 0), -2 for a row
+ * outside the readable SA. */
+TPZ_API int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
+                             const int32_t *qlen, int64_t nq, const int32_t *query_of,
+                             const int32_t *qoffset, const int64_t *row, int64_t n,
+                             const int8_t *mat625, int32_t *score, int32_t *length);
+
+/* ------------------------------------------------------------------------
+ * Whole queries: seed lookup, best-first SA walk into the capped hitlist
+ * and Smith-Waterman of every hit with gapless score >= 40 -- the work of
+ * query_find_suffixes, query_fetch_alignment_batch and
+ * query_perform_alignments (src/query.c:94-248) for a batch of queries
+ * (internal alphabet, as after run_seg + seq_2internal, src/engine.c:250-277).
+ * Hits come back per query in hitlist traversal order (gapless score
+ * descending, newest first; src/rbtree.c:653-669).  E-values and ranking are
+ * done by the caller (tpz_karlin, output_top_hits).
+ * ------------------------------------------------------------------------ */
+#define TPZ_SEARCH_MAX_QLEN 1024
+
+typedef struct {
+    int32_t num_hits;         /* -H (hitlist capacity 1.5*H for queries > 3000) */
+    int32_t gap_open;         /* -o */
+    int32_t gap_extend;       /* -e */
+    int32_t min_hit_length;   /* -l */
+    int32_t seeds;            /* -S: counted pops per query */
+    int32_t alignments;       /* -A: hitlist capacity */
+    const int8_t *mat625;     /* substitution matrix (host) */
+    int64_t trace_pops;       /* record up to this many pops per query (0: none) */
+} tpz_search_opts;
+
+typedef struct {
+    int64_t nq, nhits_total;
+    const int64_t *hit_off;                  /* nq + 1 */
+    const int64_t *npops, *ncounted;         /* nq */
+    const int32_t *status;                   /* nq, TPZ_Q_* bits */
+    const int32_t *protein, *gapless_score, *gapless_length, *suffix_offset;
+    const int32_t *rawscore, *qend, *send, *sw_status;   /* per hit, TPZ_SW_* */
+    const int64_t *trace_n;                  /* nq (when trace_pops > 0) */
+    const int64_t *trace_row;                /* nq * trace_pops */
+    const int32_t *trace_off, *trace_score, *trace_len, *trace_counted;
+} tpz_search_result;
+
+TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
+                             const int32_t *qlen, int64_t nq, const tpz_search_opts *opts,
+                             tpz_search_result **out);
+TPZ_API void tpz_search_result_free(tpz_search_result *r);
+
+/* bitscore and E-value of a raw score exactly as align_using_ssw_profile
+ * computes them with the C library's log/exp (src/ssw_wrapper.c:179-183,
+ * :239-242); db_size = Tsize - Psize and db_proteins = Psize unless given
+ * (src/engine.c:52-58). */
+TPZ_API void tpz_karlin(int32_t qlen, uint64_t db_size, uint64_t db_proteins, double lambda,
+                        double k, double H, int32_t raw, double *bitscore, double *evalue);
 
 /* Roofline probe (no reference counterpart): `blocks` x 256 threads, each
  * running 8 independent chains of `iters` __viaddmax_s16x2 ops; writes one

@@ -1,0 +1,511 @@
+// search_host.cu -- index residency and the host side of the search C ABI.
+#include <math.h>
+#include <stddef.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "search_internal.cuh"
+
+using tpz::search::Cursor;
+using tpz::search::DevIndex;
+using tpz::search::Hit;
+using tpz::search::PopRec;
+using tpz::search::QueryOut;
+
+struct tpz_index {
+    int dev = 0;
+    DevIndex d;
+    std::vector<void *> mem;
+    int64_t bytes = 0;
+    std::vector<int64_t> pstart;   // host copy, Psize + 1
+};
+
+namespace {
+
+constexpr char kInternalToAA[] = "ACMLJIVTSKRQZEDBNHYFWXP*G";
+constexpr char kMatrixOrder[] = "ARNDCQEGHILKMFPSTWYVBJZX*";
+
+// internal alphabet byte -> matrix index (aa_table2, src/lexicographical.h:19-33)
+void internal_map(int8_t out[128]) {
+    for (int i = 0; i < 128; ++i) out[i] = 23;
+    for (int i = 0; i < 25; ++i) {
+        const int m = (int)(strchr(kMatrixOrder, kInternalToAA[i]) - kMatrixOrder);
+        out['A' + i] = (int8_t)m;
+        out['a' + i] = (int8_t)m;
+    }
+}
+
+// 25x25 substitution table indexed by internal letters (subject row, query col)
+void internal_sub(const int8_t *mat, int8_t out[625]) {
+    int8_t m[128];
+    internal_map(m);
+    for (int t = 0; t < 25; ++t)
+        for (int q = 0; q < 25; ++q) out[t * 25 + q] = mat[m['A' + t] * 25 + m['A' + q]];
+}
+
+int dalloc(tpz_index *ix, void **p, size_t bytes) {
+    TPZ_CUDA(cudaMalloc(p, bytes));
+    ix->mem.push_back(*p);
+    ix->bytes += (int64_t)bytes;
+    return TPZ_OK;
+}
+
+struct DevBuf {
+    std::vector<void *> ptrs;
+    ~DevBuf() { for (void *p : ptrs) cudaFree(p); }
+    template <class T>
+    int alloc(T **p, size_t count) {
+        void *q = nullptr;
+        TPZ_CUDA(cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)));
+        ptrs.push_back(q);
+        *p = (T *)q;
+        return TPZ_OK;
+    }
+};
+
+__global__ void sa_range_check_kernel(const int64_t *SA, int64_t Tsize, int *bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < Tsize;
+         i += (int64_t)gridDim.x * blockDim.x)
+        if (SA[i] < 0 || SA[i] >= Tsize) *bad = 1;
+}
+
+struct PackArgs {
+    const Hit *hits;        // nq * max_cap
+    const QueryOut *qout;
+    const int64_t *hit_off; // nq + 1
+    const int64_t *qoff;
+    const int32_t *qlen;
+    const int64_t *pstart;
+    int nq, max_cap;
+    int32_t *protein, *gs, *gl, *so, *sw_status;
+    // SW pairs
+    int64_t *pq_off, *ps_off;
+    int32_t *pq_len, *ps_len, *p_hit;
+    int32_t *npairs;
+};
+
+// packs the per-query hit lists and lists the SW pairs (gapless >= 40)
+__global__ void pack_hits_kernel(PackArgs a) {
+    const int q = blockIdx.x;
+    const int n = a.qout[q].nhits;
+    const int64_t base = a.hit_off[q];
+    for (int h = threadIdx.x; h < n; h += blockDim.x) {
+        const Hit x = a.hits[(int64_t)q * a.max_cap + h];
+        const int64_t o = base + h;
+        a.protein[o] = x.protein;
+        a.gs[o] = x.gapless_score;
+        a.gl[o] = x.gapless_length;
+        a.so[o] = x.suffix_offset;
+        if (x.gapless_score < 40) {
+            a.sw_status[o] = TPZ_SW_GAPLESS_LOW;
+        } else {
+            const int k = atomicAdd(a.npairs, 1);
+            a.pq_off[k] = a.qoff[q];
+            a.pq_len[k] = a.qlen[q];
+            a.ps_off[k] = a.pstart[x.protein];
+            a.ps_len[k] = (int32_t)(a.pstart[x.protein + 1] - a.pstart[x.protein] - 1);
+            a.p_hit[k] = (int32_t)o;
+        }
+    }
+}
+
+__global__ void scatter_sw_kernel(int64_t n, const int32_t *p_hit, const int32_t *sc,
+                                  const int32_t *re, const int32_t *rd, const int32_t *st,
+                                  int32_t *raw, int32_t *send, int32_t *qend, int32_t *sw_status) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int h = p_hit[k];
+        raw[h] = sc[k];
+        send[h] = re[k];
+        qend[h] = rd[k];
+        sw_status[h] = st[k];
+    }
+}
+
+struct ResultHolder {
+    tpz_search_result r{};
+    std::vector<int64_t> hit_off, npops, ncounted, trace_n, trace_row;
+    std::vector<int32_t> status, protein, gs, gl, so, raw, qend, send, sw_status;
+    std::vector<int32_t> trace_off, trace_score, trace_len, trace_counted;
+};
+
+bool letters_ok(const char *s, int64_t n) {
+    for (int64_t i = 0; i < n; ++i)
+        if (s[i] < 'A' || s[i] > 'Y') return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpz_index_create(const uint8_t *T, int64_t Tsize, const int64_t *SA, const void *ind,
+                     int64_t Psize, tpz_index **out) {
+    using namespace tpz::search;
+    if (!T || !SA || !ind || !out || Tsize < 1 || Psize < 1 || Psize > INT32_MAX - 1) {
+        tpz::set_error("tpz_index_create: bad arguments");
+        return TPZ_E_ARG;
+    }
+    *out = nullptr;
+    // .ind must tile T exactly: protein p at [start, start+len) then '\n'
+    struct Rec { uint64_t hs, ps; int32_t hl, pl; };
+    const Rec *rec = (const Rec *)ind;
+    std::vector<int64_t> pstart(Psize + 1);
+    int64_t run = 0;
+    for (int64_t p = 0; p < Psize; ++p) {
+        if ((int64_t)rec[p].ps != run || rec[p].pl < 0 || run + rec[p].pl >= Tsize ||
+            T[run + rec[p].pl] != '\n') {
+            char buf[160];
+            snprintf(buf, sizeof buf, "tpz_index_create: .ind record %lld does not match the text",
+                     (long long)p);
+            tpz::set_error(buf);
+            return TPZ_E_ARG;
+        }
+        pstart[p] = run;
+        run += rec[p].pl + 1;
+    }
+    if (run != Tsize) {
+        tpz::set_error("tpz_index_create: .ind does not cover the text");
+        return TPZ_E_ARG;
+    }
+    pstart[Psize] = Tsize;
+    for (int64_t i = 0; i < Tsize; ++i) {
+        const uint8_t c = T[i];
+        if (c != '\n' && (c < 'A' || c > 'Y')) {
+            tpz::set_error("tpz_index_create: text byte outside the internal alphabet");
+            return TPZ_E_ARG;
+        }
+    }
+
+    tpz_index *ix = new tpz_index();
+    TPZ_CUDA(cudaGetDevice(&ix->dev));
+    auto fail = [&](int rc) { tpz_index_destroy(ix); return rc; };
+    const int64_t sa_rows = ((Tsize * 8 + 4095) / 4096) * 4096 / 8;
+    const int64_t nblocks = (Tsize + 63) / 64;
+    uint8_t *dT; int64_t *dSA, *dps, *dlb; uint32_t *dnl;
+    int rc;
+    if ((rc = dalloc(ix, (void **)&dT, Tsize + 128))) return fail(rc);
+    if ((rc = dalloc(ix, (void **)&dSA, sa_rows * 8))) return fail(rc);
+    if ((rc = dalloc(ix, (void **)&dps, (Psize + 1) * 8))) return fail(rc);
+    if ((rc = dalloc(ix, (void **)&dnl, (nblocks + 1) * 4))) return fail(rc);
+    if ((rc = dalloc(ix, (void **)&dlb, (kCodes + 1) * 8))) return fail(rc);
+    if (cudaMemset(dT + Tsize, '\n', 128) != cudaSuccess ||
+        cudaMemcpy(dT, T, Tsize, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(dSA, 0, sa_rows * 8) != cudaSuccess ||
+        cudaMemcpy(dSA, SA, Tsize * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dps, pstart.data(), (Psize + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create copies"));
+    int *dbad;
+    if ((rc = dalloc(ix, (void **)&dbad, 4))) return fail(rc);
+    cudaMemset(dbad, 0, 4);
+    const int nsm = tpz::sm_count();
+    // every SA entry must index T before any kernel dereferences T[SA[r]]
+    sa_range_check_kernel<<<nsm * 8, 256>>>(dSA, Tsize, dbad);
+    int bad = 0;
+    if (cudaMemcpy(&bad, dbad, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create SA check"));
+    if (bad) {
+        tpz::set_error("tpz_index_create: SA entry outside [0, Tsize)");
+        return fail(TPZ_E_ARG);
+    }
+    nl_block_count_kernel<<<nsm * 8, 256>>>(dT, Tsize, nblocks, dnl);
+    lb_build_kernel<<<nsm * 8, 256>>>(dT, Tsize, dSA, dlb);
+    std::vector<uint32_t> cnt(nblocks + 1, 0);
+    if (cudaMemcpy(cnt.data(), dnl, nblocks * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create tables"));
+    uint32_t acc = 0;
+    for (int64_t b = 0; b <= nblocks; ++b) {
+        const uint32_t c = b < nblocks ? cnt[b] : 0;
+        cnt[b] = acc;
+        acc += c;
+    }
+    if (cudaMemcpy(dnl, cnt.data(), (nblocks + 1) * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create nl"));
+    ix->d.Tsize = Tsize; ix->d.Psize = Psize; ix->d.sa_rows = sa_rows;
+    ix->d.T = dT; ix->d.SA = dSA; ix->d.pstart = dps; ix->d.nl = dnl; ix->d.lb = dlb;
+    ix->pstart.swap(pstart);
+    *out = ix;
+    return TPZ_OK;
+}
+
+void tpz_index_destroy(tpz_index *ix) {
+    if (!ix) return;
+    for (void *p : ix->mem) cudaFree(p);
+    delete ix;
+}
+
+int64_t tpz_index_device_bytes(const tpz_index *ix) { return ix ? ix->bytes : 0; }
+
+int tpz_sa_search_batch(const tpz_index *ix, const char *pcat, const int64_t *poff,
+                        const int32_t *plen, int64_t n, int64_t *idx) {
+    if (!ix || n < 0) { tpz::set_error("tpz_sa_search_batch: bad arguments"); return TPZ_E_ARG; }
+    if (n == 0) return TPZ_OK;
+    int64_t bytes = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (plen[i] < 1 || poff[i] < 0 || !letters_ok(pcat + poff[i], plen[i])) {
+            tpz::set_error("tpz_sa_search_batch: pattern must be >= 1 internal letters 'A'..'Y'");
+            return TPZ_E_ARG;
+        }
+        bytes = std::max<int64_t>(bytes, poff[i] + plen[i]);
+    }
+    DevBuf b;
+    uint8_t *dp; int64_t *doff, *dout; int32_t *dlen;
+    int rc;
+    if ((rc = b.alloc(&dp, bytes)) || (rc = b.alloc(&doff, n)) || (rc = b.alloc(&dout, n)) ||
+        (rc = b.alloc(&dlen, n)))
+        return rc;
+    TPZ_CUDA(cudaMemcpy(dp, pcat, bytes, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(doff, poff, 8 * n, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dlen, plen, 4 * n, cudaMemcpyHostToDevice));
+    tpz::search::lower_bound_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256>>>(
+        ix->d, dp, doff, dlen, n, dout);
+    TPZ_CUDA(cudaGetLastError());
+    TPZ_CUDA(cudaMemcpy(idx, dout, 8 * n, cudaMemcpyDeviceToHost));
+    return TPZ_OK;
+}
+
+int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
+                     const int32_t *qlen, int64_t nq, const int32_t *query_of,
+                     const int32_t *qoffset, const int64_t *row, int64_t n, const int8_t *mat625,
+                     int32_t *score, int32_t *length) {
+    if (!ix || nq < 1 || n < 0 || !mat625) { tpz::set_error("tpz_sa_hsp_batch: bad arguments"); return TPZ_E_ARG; }
+    if (n == 0) return TPZ_OK;
+    int64_t bytes = 0;
+    for (int64_t q = 0; q < nq; ++q) {
+        if (qlen[q] < 1 || qoff[q] < 0 || !letters_ok(qcat + qoff[q], qlen[q])) {
+            tpz::set_error("tpz_sa_hsp_batch: queries must be internal letters 'A'..'Y'");
+            return TPZ_E_ARG;
+        }
+        bytes = std::max<int64_t>(bytes, qoff[q] + qlen[q]);
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (query_of[i] < 0 || query_of[i] >= nq || qoffset[i] < 0 || qoffset[i] >= qlen[query_of[i]]) {
+            tpz::set_error("tpz_sa_hsp_batch: (query, offset) out of range");
+            return TPZ_E_ARG;
+        }
+    int8_t sub[625];
+    internal_sub(mat625, sub);
+    DevBuf b;
+    uint8_t *dq; int64_t *dqo, *drow; int32_t *dql, *dqf, *doff, *dsc, *dln; int8_t *dsub;
+    int rc;
+    if ((rc = b.alloc(&dq, bytes)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
+        (rc = b.alloc(&dqf, n)) || (rc = b.alloc(&doff, n)) || (rc = b.alloc(&drow, n)) ||
+        (rc = b.alloc(&dsc, n)) || (rc = b.alloc(&dln, n)) || (rc = b.alloc(&dsub, 625)))
+        return rc;
+    TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dqo, qoff, 8 * nq, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dql, qlen, 4 * nq, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dqf, query_of, 4 * n, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(doff, qoffset, 4 * n, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(drow, row, 8 * n, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dsub, sub, 625, cudaMemcpyHostToDevice));
+    tpz::search::hsp_batch_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256>>>(
+        ix->d, dq, dqo, dql, dqf, doff, drow, n, dsub, dsc, dln);
+    TPZ_CUDA(cudaGetLastError());
+    TPZ_CUDA(cudaMemcpy(score, dsc, 4 * n, cudaMemcpyDeviceToHost));
+    TPZ_CUDA(cudaMemcpy(length, dln, 4 * n, cudaMemcpyDeviceToHost));
+    return TPZ_OK;
+}
+
+int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
+                     const int32_t *qlen, int64_t nq, const tpz_search_opts *o,
+                     tpz_search_result **out) {
+    using namespace tpz::search;
+    if (!ix || !o || !out || nq < 1 || nq > INT32_MAX / 2 || !o->mat625) {
+        tpz::set_error("tpz_search_batch: bad arguments");
+        return TPZ_E_ARG;
+    }
+    *out = nullptr;
+    if (!(o->gap_open > o->gap_extend && o->gap_extend >= 0 && o->gap_open <= 255) ||
+        o->min_hit_length < 1 || o->seeds < 1 || o->alignments < 1 || o->num_hits < 1 ||
+        o->trace_pops < 0) {
+        tpz::set_error("tpz_search_batch: invalid options (need 255 >= gap_open > gap_extend >= 0, "
+                       "min_hit_length/seeds/alignments/num_hits >= 1)");
+        return TPZ_E_ARG;
+    }
+    int maxm = 0;
+    for (int i = 0; i < 625; ++i) maxm = std::max<int>(maxm, o->mat625[i]);
+    if (255 * maxm >= kSMax) { tpz::set_error("tpz_search_batch: matrix entries too large"); return TPZ_E_ARG; }
+
+    std::vector<int64_t> pos_base(nq + 1, 0), cur_base(nq + 1, 0);
+    std::vector<int32_t> qstatus(nq, 0), qlen_eff(nq);
+    int64_t bytes = 0;
+    int max_cap = 1, max_cursors = 1;
+    for (int64_t q = 0; q < nq; ++q) {
+        if (qlen[q] < 0 || qoff[q] < 0 || !letters_ok(qcat + qoff[q], qlen[q])) {
+            tpz::set_error("tpz_search_batch: queries must be internal letters 'A'..'Y'");
+            return TPZ_E_ARG;
+        }
+        bytes = std::max<int64_t>(bytes, qoff[q] + qlen[q]);
+        qlen_eff[q] = qlen[q];
+        if (qlen[q] > TPZ_SEARCH_MAX_QLEN) { qstatus[q] |= TPZ_Q_TOO_LONG; qlen_eff[q] = 0; }
+        const int64_t np = std::max(0, qlen_eff[q] - o->min_hit_length);
+        pos_base[q + 1] = pos_base[q] + np;
+        cur_base[q + 1] = 2 * pos_base[q + 1];
+        max_cursors = std::max<int>(max_cursors, (int)(2 * np));
+        const int cap = qlen[q] > 3000 ? (int)(1.5 * o->num_hits) : o->alignments;
+        max_cap = std::max(max_cap, cap);
+    }
+    const int64_t npos = pos_base[nq];
+    int hash_size = 16;
+    while (hash_size < 2 * (max_cap + 1)) hash_size <<= 1;
+    auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t ns = (size_t)max_cap + 1;
+    const size_t per_q = al(4 * (size_t)max_cursors) + al(4 * (size_t)kSMax) + al(8 * (kSMax / 64)) +
+                         7 * al(4 * ns) + 2 * al(4 * (size_t)kSMax) + al(8 * (kSMax / 64)) +
+                         2 * al(4 * (size_t)hash_size);
+
+    int8_t sub[625], xmap[128];
+    internal_sub(o->mat625, sub);
+    internal_map(xmap);
+
+    DevBuf b;
+    uint8_t *dq, *dscratch; int64_t *dqo, *dpb, *dcb; int32_t *dql, *dqs; int8_t *dsub;
+    Cursor *dcur; Hit *dhits; QueryOut *dqout; PopRec *dtrace = nullptr;
+    int rc;
+    if ((rc = b.alloc(&dq, bytes + 1)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
+        (rc = b.alloc(&dpb, nq + 1)) || (rc = b.alloc(&dcb, nq + 1)) || (rc = b.alloc(&dqs, nq)) ||
+        (rc = b.alloc(&dsub, 625)) || (rc = b.alloc(&dcur, 2 * npos + 1)) ||
+        (rc = b.alloc(&dscratch, per_q * nq)) || (rc = b.alloc(&dhits, (size_t)nq * max_cap)) ||
+        (rc = b.alloc(&dqout, nq)))
+        return rc;
+    if (o->trace_pops > 0 && (rc = b.alloc(&dtrace, (size_t)nq * o->trace_pops))) return rc;
+    TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dqo, qoff, 8 * nq, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dql, qlen_eff.data(), 4 * nq, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dpb, pos_base.data(), 8 * (nq + 1), cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dcb, cur_base.data(), 8 * (nq + 1), cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dqs, qstatus.data(), 4 * nq, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(dsub, sub, 625, cudaMemcpyHostToDevice));
+
+    const int nsm = tpz::sm_count();
+    if (npos > 0) {
+        SeedArgs sa;
+        sa.qcat = dq; sa.qoff = dqo; sa.qlen = dql; sa.pos_base = dpb; sa.nq = (int)nq;
+        sa.npos = npos; sa.sub = dsub; sa.cursors = dcur; sa.lb_out = nullptr; sa.qstatus = dqs;
+        seed_kernel<<<(unsigned)std::min<int64_t>((npos + 127) / 128, (int64_t)nsm * 16), 128>>>(ix->d, sa);
+    }
+    WalkArgs wa;
+    wa.qcat = dq; wa.qoff = dqo; wa.qlen = dql; wa.nq = (int)nq; wa.cursor_base = dcb;
+    wa.cursors = dcur; wa.sub = dsub; wa.min_hit_length = o->min_hit_length;
+    wa.seeds = o->seeds; wa.alignments = o->alignments; wa.num_hits = o->num_hits;
+    wa.max_cap = max_cap; wa.hash_size = hash_size; wa.max_cursors = max_cursors;
+    wa.scratch = dscratch; wa.scratch_per_query = per_q; wa.hits = dhits; wa.qout = dqout;
+    wa.qstatus = dqs; wa.trace = dtrace; wa.trace_cap = o->trace_pops;
+    walk_kernel<<<(unsigned)((nq + 31) / 32), 32>>>(ix->d, wa);
+    TPZ_CUDA(cudaGetLastError());
+
+    ResultHolder *R = new ResultHolder();
+    std::vector<QueryOut> qo(nq);
+    auto bail = [&](int code) { delete R; return code; };
+    if (cudaMemcpy(qo.data(), dqout, sizeof(QueryOut) * nq, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch walk"));
+    R->hit_off.assign(nq + 1, 0);
+    R->npops.resize(nq); R->ncounted.resize(nq); R->status.resize(nq);
+    for (int64_t q = 0; q < nq; ++q) {
+        R->hit_off[q + 1] = R->hit_off[q] + qo[q].nhits;
+        R->npops[q] = qo[q].npops;
+        R->ncounted[q] = qo[q].ncounted;
+        R->status[q] = qo[q].status | qstatus[q];
+    }
+    const int64_t nh = R->hit_off[nq];
+    for (auto *v : {&R->protein, &R->gs, &R->gl, &R->so, &R->raw, &R->qend, &R->send, &R->sw_status})
+        v->assign(nh, -1);
+
+    if (nh > 0) {
+        int64_t *dho, *pq_off, *ps_off; int32_t *pprot, *pgs, *pgl, *pso, *psw, *pq_len, *ps_len, *p_hit, *dnp;
+        int32_t *sc, *re, *rd, *st, *raw, *qend, *send;
+        if ((rc = b.alloc(&dho, nq + 1)) || (rc = b.alloc(&pprot, nh)) || (rc = b.alloc(&pgs, nh)) ||
+            (rc = b.alloc(&pgl, nh)) || (rc = b.alloc(&pso, nh)) || (rc = b.alloc(&psw, nh)) ||
+            (rc = b.alloc(&pq_off, nh)) || (rc = b.alloc(&ps_off, nh)) || (rc = b.alloc(&pq_len, nh)) ||
+            (rc = b.alloc(&ps_len, nh)) || (rc = b.alloc(&p_hit, nh)) || (rc = b.alloc(&dnp, 1)) ||
+            (rc = b.alloc(&sc, nh)) || (rc = b.alloc(&re, nh)) || (rc = b.alloc(&rd, nh)) ||
+            (rc = b.alloc(&st, nh)) || (rc = b.alloc(&raw, nh)) || (rc = b.alloc(&qend, nh)) ||
+            (rc = b.alloc(&send, nh)))
+            return bail(rc);
+        if (cudaMemcpy(dho, R->hit_off.data(), 8 * (nq + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(dnp, 0, 4) != cudaSuccess || cudaMemset(raw, 0xFF, 4 * nh) != cudaSuccess ||
+            cudaMemset(qend, 0xFF, 4 * nh) != cudaSuccess || cudaMemset(send, 0xFF, 4 * nh) != cudaSuccess)
+            return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch pack"));
+        PackArgs pa;
+        pa.hits = dhits; pa.qout = dqout; pa.hit_off = dho; pa.qoff = dqo; pa.qlen = dql;
+        pa.pstart = ix->d.pstart; pa.nq = (int)nq; pa.max_cap = max_cap;
+        pa.protein = pprot; pa.gs = pgs; pa.gl = pgl; pa.so = pso; pa.sw_status = psw;
+        pa.pq_off = pq_off; pa.ps_off = ps_off; pa.pq_len = pq_len; pa.ps_len = ps_len;
+        pa.p_hit = p_hit; pa.npairs = dnp;
+        pack_hits_kernel<<<(unsigned)nq, 256>>>(pa);
+        int32_t npairs = 0;
+        if (cudaMemcpy(&npairs, dnp, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch pairs"));
+        if (npairs > 0) {
+            rc = tpz::sw::batch_device_x(npairs, (const int8_t *)dq, pq_off, pq_len,
+                                         (const int8_t *)ix->d.T, ps_off, ps_len, o->mat625,
+                                         o->gap_open, o->gap_extend, sc, re, rd, st, 0, xmap, xmap);
+            if (rc) return bail(rc);
+            scatter_sw_kernel<<<(unsigned)std::min<int64_t>((npairs + 255) / 256, 4096), 256>>>(
+                npairs, p_hit, sc, re, rd, st, raw, send, qend, psw);
+        }
+        if (cudaMemcpy(R->protein.data(), pprot, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->gs.data(), pgs, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->gl.data(), pgl, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->so.data(), pso, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->sw_status.data(), psw, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->raw.data(), raw, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->qend.data(), qend, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(R->send.data(), send, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch results"));
+    }
+    if (o->trace_pops > 0) {
+        std::vector<PopRec> tr((size_t)nq * o->trace_pops);
+        if (cudaMemcpy(tr.data(), dtrace, sizeof(PopRec) * tr.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch trace"));
+        R->trace_n.resize(nq);
+        R->trace_row.resize(tr.size()); R->trace_off.resize(tr.size());
+        R->trace_score.resize(tr.size()); R->trace_len.resize(tr.size()); R->trace_counted.resize(tr.size());
+        for (size_t i = 0; i < tr.size(); ++i) {
+            R->trace_row[i] = tr[i].row; R->trace_off[i] = tr[i].off; R->trace_score[i] = tr[i].score;
+            R->trace_len[i] = tr[i].len; R->trace_counted[i] = tr[i].counted;
+        }
+        for (int64_t q = 0; q < nq; ++q) R->trace_n[q] = std::min<int64_t>(qo[q].npops, o->trace_pops);
+    }
+    tpz_search_result &r = R->r;
+    r.nq = nq; r.nhits_total = nh; r.hit_off = R->hit_off.data(); r.npops = R->npops.data();
+    r.ncounted = R->ncounted.data(); r.status = R->status.data(); r.protein = R->protein.data();
+    r.gapless_score = R->gs.data(); r.gapless_length = R->gl.data(); r.suffix_offset = R->so.data();
+    r.rawscore = R->raw.data(); r.qend = R->qend.data(); r.send = R->send.data();
+    r.sw_status = R->sw_status.data();
+    r.trace_n = o->trace_pops > 0 ? R->trace_n.data() : nullptr;
+    r.trace_row = o->trace_pops > 0 ? R->trace_row.data() : nullptr;
+    r.trace_off = o->trace_pops > 0 ? R->trace_off.data() : nullptr;
+    r.trace_score = o->trace_pops > 0 ? R->trace_score.data() : nullptr;
+    r.trace_len = o->trace_pops > 0 ? R->trace_len.data() : nullptr;
+    r.trace_counted = o->trace_pops > 0 ? R->trace_counted.data() : nullptr;
+    TPZ_CUDA(cudaDeviceSynchronize());
+    *out = &R->r;
+    return TPZ_OK;
+}
+
+void tpz_search_result_free(tpz_search_result *r) {
+    if (!r) return;
+    ResultHolder *h = reinterpret_cast<ResultHolder *>(reinterpret_cast<char *>(r) -
+                                                       offsetof(ResultHolder, r));
+    delete h;
+}
+
+void tpz_karlin(int32_t qlen, uint64_t db_size, uint64_t db_proteins, double lambda, double k,
+                double H, int32_t raw, double *bitscore, double *evalue) {
+    const double correction = log(k * qlen * db_size) / H;
+    const double corrected_q = fmax(qlen - correction, 1.0);
+    const double corrected_db = fmax(db_size - (correction * db_proteins), 1.0);
+    double bits = (lambda * raw - log(k));
+    double ev = corrected_q * corrected_db * exp(-bits);
+    ev = ev > 1.0e-180 ? ev : 0.0;
+    *bitscore = bits / M_LN2;
+    *evalue = ev;
+}
+
+}  // extern "C"

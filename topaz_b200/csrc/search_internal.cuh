@@ -1,0 +1,95 @@
+// search_internal.cuh -- device structures of the search path.
+#pragma once
+
+#include "tpz_common.cuh"
+
+namespace tpz {
+namespace search {
+
+constexpr int kK = 5;                       // prefix-table width (symbols)
+constexpr int64_t kCodes = 11881376;        // 26^5
+constexpr int kSMax = 4352;                 // gapless scores are < 255*17+1 <= kSMax
+
+struct DevIndex {
+    int64_t Tsize = 0, Psize = 0, sa_rows = 0;
+    const uint8_t *T = nullptr;
+    const int64_t *SA = nullptr;
+    const int64_t *pstart = nullptr;    // Psize + 1
+    const uint32_t *nl = nullptr;       // per 64-byte block
+    const int64_t *lb = nullptr;        // kCodes + 1
+};
+
+struct Cursor {
+    int64_t row;
+    int32_t off, dir, score, len;
+};
+
+struct Hit {
+    int32_t protein, gapless_score, gapless_length, suffix_offset;
+};
+
+struct PopRec {
+    int64_t row;
+    int32_t off, score, len, counted;
+};
+
+struct QueryOut {
+    int64_t npops, ncounted;
+    int32_t nhits, status;
+};
+
+struct SeedArgs {
+    const uint8_t *qcat;
+    const int64_t *qoff;
+    const int32_t *qlen;
+    const int64_t *pos_base;   // nq + 1: searched positions before each query
+    int nq;
+    int64_t npos;
+    const int8_t *sub;         // 25x25 by internal letter (subject row, query col)
+    Cursor *cursors;           // 2 per position
+    int64_t *lb_out;           // optional: bound per position (-2 skipped)
+    int32_t *qstatus;          // per query status bits
+};
+
+struct WalkArgs {
+    const uint8_t *qcat;
+    const int64_t *qoff;
+    const int32_t *qlen;
+    int nq;
+    const int64_t *cursor_base;   // nq + 1
+    Cursor *cursors;
+    const int8_t *sub;
+    int min_hit_length, seeds, alignments, num_hits;
+    int max_cap, hash_size, max_cursors;
+    uint8_t *scratch;
+    size_t scratch_per_query;
+    Hit *hits;                    // nq * max_cap
+    QueryOut *qout;
+    const int32_t *qstatus;
+    PopRec *trace;                // optional: nq * trace_cap
+    int64_t trace_cap;
+};
+
+__global__ void nl_block_count_kernel(const uint8_t *T, int64_t Tsize, int64_t nblocks, uint32_t *cnt);
+__global__ void lb_build_kernel(const uint8_t *T, int64_t Tsize, const int64_t *SA, int64_t *lb);
+__global__ void seed_kernel(DevIndex ix, SeedArgs a);
+__global__ void walk_kernel(DevIndex ix, WalkArgs a);
+__global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t *qoff,
+                                 const int32_t *qlen, const int32_t *query_of, const int32_t *off,
+                                 const int64_t *row, int64_t n, const int8_t *sub, int32_t *score,
+                                 int32_t *len);
+__global__ void lower_bound_kernel(DevIndex ix, const uint8_t *pcat, const int64_t *poff,
+                                   const int32_t *plen, int64_t n, int64_t *out);
+
+}  // namespace search
+
+namespace sw {
+// Batched SW over device buffers; xq/xs (128-entry maps, may be null) turn
+// query/subject bytes into matrix indices inside the kernel.
+int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                   const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
+                   int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
+                   int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs);
+}  // namespace sw
+
+}  // namespace tpz

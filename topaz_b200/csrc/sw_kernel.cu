@@ -82,7 +82,9 @@ struct Args {
     int32_t *rerun_count;
     int ssw_lanes;           // 16 (u8 pass) or 8 (i16 pass)
     int gap_open, gap_extend, bias;
+    int translate;           // 1: q/s bytes go through xq/xs first
     int8_t mat[625];
+    int8_t xq[128], xs[128]; // byte -> matrix index (internal alphabet inputs)
 };
 
 __device__ __forceinline__ uint32_t pack2(int lo, int hi) {
@@ -120,6 +122,10 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     for (int r = 0; r < R; ++r) {
         qa[r] = (i0 + r < qlA) ? qA[i0 + r] : -1;
         qb[r] = (i0 + r < qlB) ? qB[i0 + r] : -1;
+        if (a.translate) {
+            if (qa[r] >= 0) qa[r] = a.xq[qa[r] & 127];
+            if (qb[r] >= 0) qb[r] = a.xq[qb[r] & 127];
+        }
     }
     __syncwarp();
     for (int let = 0; let < 26; ++let) {
@@ -183,8 +189,12 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             inH = 0u; inF = 0u; inFm = 0u;
             // the subject letters of column k enter at lane 0 (an L1-resident
             // byte load; cheaper here than a shuffle-fed prefetch window)
-            const int la = k < slA ? sA[k] : kPadLetter;
-            const int lb = k < slB ? sB[k] : kPadLetter;
+            int la = k < slA ? sA[k] : kPadLetter;
+            int lb = k < slB ? sB[k] : kPadLetter;
+            if (a.translate) {
+                if (k < slA) la = a.xs[la & 127];
+                if (k < slB) lb = a.xs[lb & 127];
+            }
             inLet = (uint32_t)la | ((uint32_t)lb << 8);
         }
         const int j = k - lane;
@@ -484,10 +494,10 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
     return TPZ_OK;
 }
 
-int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
-                 const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
-                 int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
-                 int32_t *status, cudaStream_t st) {
+int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                   const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
+                   int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
+                   int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs) {
     g_last_launches = 0;
     if (n < 0 || n > INT32_MAX / 2 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
     if (!(go > ge && ge >= 0 && go <= 255)) {
@@ -526,6 +536,13 @@ int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t 
     for (int i = 0; i < 625; ++i) mn = std::min<int>(mn, mat[i]);
     a.bias = -mn;
     memcpy(a.mat, mat, 625);
+    a.translate = (xq && xs) ? 1 : 0;
+    memset(a.xq, 0, sizeof a.xq);
+    memset(a.xs, 0, sizeof a.xs);
+    if (a.translate) {
+        memcpy(a.xq, xq, 128);
+        memcpy(a.xs, xs, 128);
+    }
 
     int64_t launches = 0;
     TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, sizeof(int32_t), st));
@@ -538,6 +555,14 @@ int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t 
     TPZ_CUDA(cudaFreeAsync(ws, st));
     g_last_launches = launches;
     return TPZ_OK;
+}
+
+int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                 const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
+                 int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
+                 int32_t *status, cudaStream_t st) {
+    return batch_device_x(n, q, qoff, qlen, s, soff, slen, mat, go, ge, score, ref_end, read_end,
+                          status, st, nullptr, nullptr);
 }
 
 }  // namespace sw

@@ -117,3 +117,150 @@ def dpx_probe(blocks, iters, out_ptr, stream=0) -> int:
     ops = ctypes.c_int64()
     check(lib().tpz_dpx_probe(blocks, iters, out_ptr, stream, ctypes.byref(ops)))
     return ops.value
+
+
+# ------------------------------------------------------------------ search
+
+class _SearchOpts(ctypes.Structure):
+    _fields_ = [("num_hits", ctypes.c_int32), ("gap_open", ctypes.c_int32),
+                ("gap_extend", ctypes.c_int32), ("min_hit_length", ctypes.c_int32),
+                ("seeds", ctypes.c_int32), ("alignments", ctypes.c_int32),
+                ("mat625", _VP), ("trace_pops", ctypes.c_int64)]
+
+
+_P64 = ctypes.POINTER(ctypes.c_int64)
+_P32 = ctypes.POINTER(ctypes.c_int32)
+
+
+class _SearchResult(ctypes.Structure):
+    _fields_ = [("nq", ctypes.c_int64), ("nhits_total", ctypes.c_int64),
+                ("hit_off", _P64), ("npops", _P64), ("ncounted", _P64), ("status", _P32),
+                ("protein", _P32), ("gapless_score", _P32), ("gapless_length", _P32),
+                ("suffix_offset", _P32), ("rawscore", _P32), ("qend", _P32), ("send", _P32),
+                ("sw_status", _P32), ("trace_n", _P64), ("trace_row", _P64),
+                ("trace_off", _P32), ("trace_score", _P32), ("trace_len", _P32),
+                ("trace_counted", _P32)]
+
+
+def _search_sigs(L):
+    if getattr(L, "_search_sigs", False):
+        return
+    L.tpz_index_create.argtypes = [_VP, _I64, _VP, _VP, _I64, ctypes.POINTER(_VP)]
+    L.tpz_index_destroy.argtypes = [_VP]
+    L.tpz_index_device_bytes.argtypes = [_VP]
+    L.tpz_index_device_bytes.restype = ctypes.c_int64
+    L.tpz_sa_search_batch.argtypes = [_VP, _VP, _VP, _VP, _I64, _VP]
+    L.tpz_sa_hsp_batch.argtypes = [_VP, _VP, _VP, _VP, _I64, _VP, _VP, _VP, _I64, _VP, _VP, _VP]
+    L.tpz_search_batch.argtypes = [_VP, _VP, _VP, _VP, _I64, ctypes.POINTER(_SearchOpts),
+                                   ctypes.POINTER(ctypes.POINTER(_SearchResult))]
+    L.tpz_search_result_free.argtypes = [ctypes.POINTER(_SearchResult)]
+    L.tpz_karlin.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L._search_sigs = True
+
+
+def _concat(seqs):
+    """list of bytes -> (cat uint8, off int64, len int32)"""
+    lens = np.array([len(s) for s in seqs], dtype=np.int32)
+    off = np.zeros(len(seqs), dtype=np.int64)
+    if len(seqs) > 1:
+        off[1:] = np.cumsum(lens, dtype=np.int64)[:-1]
+    cat = np.frombuffer(b"".join(seqs) + b"\0", dtype=np.uint8)
+    return cat, off, lens
+
+
+class Index:
+    """A database resident in device memory (tpz_index)."""
+
+    def __init__(self, db):
+        L = lib()
+        _search_sigs(L)
+        self.db = db
+        self._T = np.ascontiguousarray(db.T, dtype=np.uint8)
+        self._SA = np.ascontiguousarray(db.SA, dtype=np.int64)
+        self._ind = np.ascontiguousarray(db.ind)
+        h = _VP()
+        check(L.tpz_index_create(_p(self._T), len(self._T), _p(self._SA), _p(self._ind),
+                                 len(self._ind), ctypes.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().tpz_index_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self):
+        return int(lib().tpz_index_device_bytes(self.handle))
+
+    def sa_search(self, patterns):
+        cat, off, lens = _concat(patterns)
+        out = np.zeros(len(patterns), dtype=np.int64)
+        check(lib().tpz_sa_search_batch(self.handle, _p(cat), _p(off), _p(lens), len(patterns),
+                                        _p(out)))
+        return out
+
+    def sa_hsp(self, queries, query_of, qoffset, row, mat):
+        cat, off, lens = _concat(queries)
+        query_of = np.ascontiguousarray(query_of, dtype=np.int32)
+        qoffset = np.ascontiguousarray(qoffset, dtype=np.int32)
+        row = np.ascontiguousarray(row, dtype=np.int64)
+        mat = np.ascontiguousarray(mat, dtype=np.int8)
+        n = len(row)
+        sc = np.zeros(n, dtype=np.int32)
+        ln = np.zeros(n, dtype=np.int32)
+        check(lib().tpz_sa_hsp_batch(self.handle, _p(cat), _p(off), _p(lens), len(queries),
+                                     _p(query_of), _p(qoffset), _p(row), n, _p(mat), _p(sc),
+                                     _p(ln)))
+        return sc, ln
+
+    def search(self, queries, mat, num_hits=100, gap_open=11, gap_extend=1, min_hit_length=5,
+               seeds=300000, alignments=5000, trace_pops=0):
+        """Runs a batch of queries (internal-alphabet bytes).  Returns a dict
+        of numpy arrays (per query: hit_off, npops, ncounted, status; per hit:
+        protein, gapless_score, gapless_length, suffix_offset, rawscore,
+        qend, send, sw_status; optional trace_*)."""
+        L = lib()
+        cat, off, lens = _concat(queries)
+        mat = np.ascontiguousarray(mat, dtype=np.int8)
+        o = _SearchOpts(num_hits, gap_open, gap_extend, min_hit_length, seeds, alignments,
+                        _p(mat), trace_pops)
+        res = ctypes.POINTER(_SearchResult)()
+        check(L.tpz_search_batch(self.handle, _p(cat), _p(off), _p(lens), len(queries),
+                                 ctypes.byref(o), ctypes.byref(res)))
+        try:
+            r = res.contents
+            nq, nh = r.nq, r.nhits_total
+
+            def arr(ptr, n):
+                return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.int64)
+
+            out = {"hit_off": arr(r.hit_off, nq + 1), "npops": arr(r.npops, nq),
+                   "ncounted": arr(r.ncounted, nq), "status": arr(r.status, nq)}
+            for k in ("protein", "gapless_score", "gapless_length", "suffix_offset", "rawscore",
+                      "qend", "send", "sw_status"):
+                out[k] = arr(getattr(r, k), nh)
+            if trace_pops:
+                out["trace_n"] = arr(r.trace_n, nq)
+                for k in ("trace_row", "trace_off", "trace_score", "trace_len", "trace_counted"):
+                    out[k] = arr(getattr(r, k), nq * trace_pops).reshape(nq, trace_pops)
+            return out
+        finally:
+            L.tpz_search_result_free(res)
+
+
+def karlin(qlen, db_size, db_proteins, raw, lam=0.267, k=0.041, H=0.14):
+    """(bitscore, evalue) as align_using_ssw_profile computes them."""
+    L = lib()
+    _search_sigs(L)
+    b, e = ctypes.c_double(), ctypes.c_double()
+    L.tpz_karlin(int(qlen), int(db_size), int(db_proteins), lam, k, H, int(raw),
+                 ctypes.byref(b), ctypes.byref(e))
+    return b.value, e.value
