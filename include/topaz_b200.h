@@ -91,6 +91,28 @@ TPZ_API int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, c
                       const int8_t *mat625, int gap_open, int gap_extend,
                       int32_t *score, int32_t *ref_end, int32_t *read_end, int32_t *status);
 
+/* Allocation-free variant of tpz_sw_batch_device, with no counterpart in the
+ * TOPAZ reference.  For callers that must not have device memory allocated
+ * on their behalf -- e.g. a server whose HBM is planned around a resident
+ * index and fixed in-flight batches, where an allocation could fail midway
+ * through a request, or a loop that cannot afford the device-wide
+ * synchronization of cudaMalloc/cudaFree.  Same arguments and results as
+ * tpz_sw_batch_device; at most TPZ_SW_NOALLOC_MAX_PAIRS pairs per call
+ * (TPZ_E_RANGE beyond).  Scratch is one static device array per device
+ * (about 0.6 MB, held until the process exits) shared by all calls: calls
+ * whose work overlaps on the GPU (other streams or threads) race on it, so
+ * order them on one stream.  All work goes to `stream`; nothing is
+ * allocated or freed.  The first call on a device does a one-time set-up
+ * (device address of the scratch array, kernel attributes) and should come
+ * before any stream capture that includes a call. */
+#define TPZ_SW_NOALLOC_MAX_PAIRS 65536
+TPZ_API int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int64_t *qoff,
+                                        const int32_t *qlen, const int8_t *s, const int64_t *soff,
+                                        const int32_t *slen, const int8_t *mat625_host,
+                                        int gap_open, int gap_extend, int32_t *score,
+                                        int32_t *ref_end, int32_t *read_end, int32_t *status,
+                                        void *stream);
+
 /* Kernel launches enqueued by the last tpz_sw_batch_* call on this thread
  * (for launch accounting). */
 TPZ_API int64_t tpz_sw_last_launches(void);

@@ -679,3 +679,152 @@ int tpz_dpx_probe(int64_t blocks, int iters, uint32_t *out, void *stream, int64_
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- allocation-free variant
+//
+// Some callers cannot let a library allocate device memory on their request
+// path: a search server that has planned its HBM around a resident index and
+// a fixed set of in-flight batches (an allocation there can fail under
+// memory pressure halfway through a request), or a host loop that must not
+// stall on the allocator -- cudaMalloc/cudaFree synchronize the device and
+// would serialize every concurrent stream.  For them the batched SW below
+// keeps its scratch (bin counts, bin cursors, the sorted pair list and the
+// rerun list) in one statically sized device array instead of a per-call
+// allocation, and enqueues everything on the caller's stream only.
+
+namespace tpz {
+namespace sw {
+
+constexpr int64_t kNoAllocMaxPairs = TPZ_SW_NOALLOC_MAX_PAIRS;
+constexpr size_t kNoAllocWords = 2 * (size_t)kBins + 2 * kRBins + kRBins + 4 + 2 * (size_t)kNoAllocMaxPairs;
+
+// One copy per device that loads the library, kept until the process exits.
+static __device__ __align__(256) int32_t g_noalloc_scratch[kNoAllocWords];
+
+struct NoAllocDev {
+    int32_t *scratch = nullptr;      // device address of g_noalloc_scratch
+    KernelFn fn[kMaxR];
+    int blocks_per_sm[kMaxR];
+};
+
+// Per-device set-up, done by the first call on each device with that device
+// current: the device address of the static scratch array (host code cannot
+// use the array's name as a device pointer) and the bin kernels' launch
+// attributes.
+static int noalloc_setup(const NoAllocDev **out) {
+    static std::mutex mu;
+    static std::vector<NoAllocDev *> per_dev;
+    int dev = 0;
+    TPZ_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, nullptr);
+    if (!per_dev[dev]) {
+        NoAllocDev *d = new NoAllocDev();
+        cudaError_t e = cudaGetSymbolAddress((void **)&d->scratch, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            delete d;
+            return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        }
+        Table<kMaxR>::fill(d->fn);
+        for (int r = 1; r <= kMaxR; ++r) {
+            e = cudaFuncSetAttribute((const void *)d->fn[r - 1],
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(r));
+            int nb = 0;
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)d->fn[r - 1], 32,
+                                                                  smem_bytes(r));
+            if (e != cudaSuccess) {
+                delete d;
+                return cuda_fail(e, "allocation-free SW set-up");
+            }
+            d->blocks_per_sm[r - 1] = std::max(1, nb);
+        }
+        per_dev[dev] = d;
+    }
+    *out = per_dev[dev];
+    return TPZ_OK;
+}
+
+static int noalloc_round(const NoAllocDev *d, Args &a, int64_t n, const int32_t *list,
+                         const int32_t *list_n, int32_t *counts, int32_t *cursor, int32_t *sorted,
+                         cudaStream_t st) {
+    const int nsm = sm_count();
+    TPZ_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * kBins, st));
+    const int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
+    bin_count_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, counts,
+                                                      a.status);
+    bin_scan_kernel<<<1, 1024, 0, st>>>(counts, cursor, const_cast<int32_t *>(a.rinfo), a.next_task);
+    bin_scatter_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, cursor,
+                                                        sorted);
+    for (int r = kMaxR; r >= 1; --r)
+        d->fn[r - 1]<<<nsm * d->blocks_per_sm[r - 1], 32, smem_bytes(r), st>>>(a);
+    TPZ_CUDA(cudaGetLastError());
+    return TPZ_OK;
+}
+
+}  // namespace sw
+}  // namespace tpz
+
+extern "C" int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int64_t *qoff,
+                                           const int32_t *qlen, const int8_t *s,
+                                           const int64_t *soff, const int32_t *slen,
+                                           const int8_t *mat625_host, int gap_open,
+                                           int gap_extend, int32_t *score, int32_t *ref_end,
+                                           int32_t *read_end, int32_t *status, void *stream) {
+    using namespace tpz::sw;
+    if (n < 0 || !mat625_host) {
+        tpz::set_error("tpz_sw_batch_device_noalloc: n < 0 or NULL matrix");
+        return TPZ_E_ARG;
+    }
+    if (n > kNoAllocMaxPairs) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "tpz_sw_batch_device_noalloc: %lld pairs exceed the fixed scratch of %lld pairs; "
+                 "split the batch or use tpz_sw_batch_device",
+                 (long long)n, (long long)kNoAllocMaxPairs);
+        tpz::set_error(buf);
+        return TPZ_E_RANGE;
+    }
+    if (!(gap_open > gap_extend && gap_extend >= 0 && gap_open <= 255)) {
+        tpz::set_error("tpz_sw_batch_device_noalloc: requires 255 >= gap_open > gap_extend >= 0");
+        return TPZ_E_ARG;
+    }
+    if (n == 0) return TPZ_OK;
+    if (!q || !qoff || !qlen || !s || !soff || !slen || !score || !ref_end || !read_end || !status) {
+        tpz::set_error("tpz_sw_batch_device_noalloc: NULL buffer");
+        return TPZ_E_ARG;
+    }
+    const NoAllocDev *d = nullptr;
+    int rc = noalloc_setup(&d);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    int32_t *counts = d->scratch;
+    int32_t *cursor = counts + kBins;
+    int32_t *rinfo = cursor + kBins;
+    int32_t *next_task = rinfo + 2 * kRBins;
+    int32_t *rerun_count = next_task + kRBins;
+    int32_t *sorted = rerun_count + 4;
+    int32_t *rerun = sorted + kNoAllocMaxPairs;
+
+    Args a;
+    a.q = q; a.qoff = qoff; a.qlen = qlen; a.s = s; a.soff = soff; a.slen = slen;
+    a.score = score; a.ref_end = ref_end; a.read_end = read_end; a.status = status;
+    a.sorted = sorted; a.rinfo = rinfo; a.next_task = next_task;
+    a.rerun = rerun; a.rerun_count = rerun_count;
+    a.gap_open = gap_open; a.gap_extend = gap_extend;
+    int mn = 0;
+    for (int i = 0; i < 625; ++i) mn = std::min<int>(mn, mat625_host[i]);
+    a.bias = -mn;
+    memcpy(a.mat, mat625_host, 625);
+    a.translate = 0;
+    memset(a.xq, 0, sizeof a.xq);
+    memset(a.xs, 0, sizeof a.xs);
+
+    // the rerun counter carries the previous call's value: clear it
+    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, sizeof(int32_t), st));
+    a.ssw_lanes = 16;
+    rc = noalloc_round(d, a, n, nullptr, nullptr, counts, cursor, sorted, st);
+    if (rc) return rc;
+    a.ssw_lanes = 8;
+    return noalloc_round(d, a, n, rerun, rerun_count, counts, cursor, sorted, st);
+}
