@@ -77,7 +77,7 @@ TPZ_API int tpz_matrix(const char *name, int8_t *out625);
  * Outputs per pair: score, ref_end (0-based subject end, -1 when score is 0),
  * read_end (0-based query end), status (TPZ_SW_*).
  * ------------------------------------------------------------------------ */
-#define TPZ_SW_MAX_QLEN 1024
+#define TPZ_SW_MAX_QLEN 8192
 #define TPZ_SW_MAX_SLEN (1 << 24)
 
 TPZ_API int tpz_sw_batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
@@ -98,7 +98,8 @@ TPZ_API int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, c
  * through a request, or a loop that cannot afford the device-wide
  * synchronization of cudaMalloc/cudaFree.  Same arguments and results as
  * tpz_sw_batch_device; at most TPZ_SW_NOALLOC_MAX_PAIRS pairs per call
- * (TPZ_E_RANGE beyond).  Scratch is one static device array per device
+ * (TPZ_E_RANGE beyond) and queries of at most TPZ_SW_NOALLOC_MAX_QLEN
+ * residues (longer ones get status TPZ_SW_INVALID).  Scratch is one static device array per device
  * (about 0.6 MB, held until the process exits) shared by all calls: calls
  * whose work overlaps on the GPU (other streams or threads) race on it, so
  * order them on one stream.  All work goes to `stream`; nothing is
@@ -106,6 +107,7 @@ TPZ_API int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, c
  * (device address of the scratch array, kernel attributes) and should come
  * before any stream capture that includes a call. */
 #define TPZ_SW_NOALLOC_MAX_PAIRS 65536
+#define TPZ_SW_NOALLOC_MAX_QLEN 1024
 TPZ_API int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int64_t *qoff,
                                         const int32_t *qlen, const int8_t *s, const int64_t *soff,
                                         const int32_t *slen, const int8_t *mat625_host,
@@ -157,7 +159,7 @@ TPZ_API int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_
  * descending, newest first; src/rbtree.c:653-669).  E-values and ranking are
  * done by the caller (tpz_karlin, output_top_hits).
  * ------------------------------------------------------------------------ */
-#define TPZ_SEARCH_MAX_QLEN 1024
+#define TPZ_SEARCH_MAX_QLEN 8192
 
 typedef struct {
     int32_t num_hits;         /* -H (hitlist capacity 1.5*H for queries > 3000) */

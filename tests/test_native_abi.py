@@ -54,5 +54,5 @@ def test_sw_rejects_bad_gaps_and_sizes_before_device_work():
         native.sw_batch_host(q, [0], [4], q, [0], [4], synth.matrix(), 1, 1)
     assert e.value.code in (-1,)                      # gap_open <= gap_extend
     with pytest.raises(native.TopazError) as e:
-        native.sw_batch_host(np.zeros(2000, np.int8), [0], [2000], q, [0], [4], synth.matrix())
+        native.sw_batch_host(np.zeros(9000, np.int8), [0], [9000], q, [0], [4], synth.matrix())
     assert e.value.code == -4                         # qlen above the limit

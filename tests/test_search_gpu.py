@@ -62,7 +62,7 @@ def test_search_matches_reference_golden(cuda, golden_search, variant):
 @pytest.fixture(scope="module")
 def fresh():
     prot = synth.protein_db(3000, seed=31)
-    qs = synth.search_queries(prot, 24, 6, seed=32, hi=1024)
+    qs = synth.search_queries(prot, 24, 6, seed=32, hi=2600)
     db = make_db(prot)
     return db, [ab.aa_to_internal(s).tobytes() for s in qs.seqs]
 

@@ -101,3 +101,38 @@ def test_sw_full_size_sample_and_order_independence(cuda):
     psr = synth.PairSet(ps.q, ps.qoff[rev], ps.qlen[rev], ps.s, ps.soff[rev], ps.slen[rev], 0)
     got_r = _run_dev(cuda, psr, mat)
     assert (got_r[:, ::-1] == got).all()
+
+
+def test_sw_long_queries_multi_stripe(cuda):
+    # queries longer than one 1024-row stripe: random, homologous (u8
+    # saturation -> i16 pass) and W-runs near / past the 16-bit limit (the
+    # 32-bit rerun): 2977 W = 32747 (kept), 3000 W = 33000 (dropped)
+    rng = np.random.default_rng(21)
+    W = 17  # W in ARNDCQEGHILKMFPSTWYVBJZX*
+    qs, ss = [], []
+    for L in (1025, 1500, 2048, 2049, 3000, 4100):
+        q = rng.integers(0, 20, L).astype(np.int8)
+        qs.append(q); ss.append(rng.integers(0, 20, int(rng.integers(1, 1500))).astype(np.int8))
+        qs.append(q); ss.append(np.concatenate([rng.integers(0, 20, 30).astype(np.int8), q[100:900]]))
+    for L in (2900, 2977, 3000):
+        q = np.full(L, W, np.int8)
+        qs.append(q); ss.append(q.copy())
+    ps = synth.sw_pairs(60, seed=3, q_range=(1025, 8192), q_median=2500, s_range=(0, 3000))
+    qs += [ps.q[o:o + l] for o, l in zip(ps.qoff, ps.qlen)]
+    ss += [ps.s[o:o + l] for o, l in zip(ps.soff, ps.slen)]
+    # and short pairs in the same batch
+    short = synth.sw_pairs(300, seed=4)
+    qs += [short.q[o:o + l] for o, l in zip(short.qoff, short.qlen)]
+    ss += [short.s[o:o + l] for o, l in zip(short.soff, short.slen)]
+    ql = np.array([len(x) for x in qs], np.int32); sl = np.array([len(x) for x in ss], np.int32)
+    qo = np.concatenate([[0], np.cumsum(ql)[:-1]]).astype(np.int64)
+    so = np.concatenate([[0], np.cumsum(sl)[:-1]]).astype(np.int64)
+    ps = synth.PairSet(np.concatenate(qs), qo, ql, np.concatenate(ss), so, sl, 0)
+    mat = synth.matrix("BLOSUM62")
+    got = _run_dev(cuda, ps, mat)
+    ref = np.stack(oracle.oracle_sw(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat))
+    bad = np.flatnonzero((got != ref).any(axis=0))
+    assert bad.size == 0, (bad[:5], got[:, bad[:5]], ref[:, bad[:5]], ps.qlen[bad[:5]])
+    assert (ref[0] == 32747).any() and (ref[3] == native.TPZ_SW_DROPPED).any()
+    host = np.stack(native.sw_batch_host(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat))
+    assert (host == ref).all()

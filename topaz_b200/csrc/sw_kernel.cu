@@ -51,8 +51,11 @@
 namespace tpz {
 namespace sw {
 
-constexpr int kMaxR = 32;           // rows per lane -> qlen <= 1024
-constexpr int kRBins = kMaxR;
+constexpr int kMaxR = 32;           // rows per lane; one stripe = 32 lanes x R rows
+constexpr int kStripeRows = 32 * kMaxR;
+constexpr int kMaxStripes = TPZ_SW_MAX_QLEN / kStripeRows;
+// row bins: b < 32 -> R = b+1, one stripe; b = 32..38 -> R = 32, b-30 stripes
+constexpr int kRBins = 40;
 constexpr int kSBins = 256;         // subject-length buckets (32 residues each)
 constexpr int kBins = kRBins * kSBins;
 constexpr int kPadLetter = 25;      // subject column past a pair's end
@@ -83,6 +86,11 @@ struct Args {
     int ssw_lanes;           // 16 (u8 pass) or 8 (i16 pass)
     int gap_open, gap_extend, bias;
     int translate;           // 1: q/s bytes go through xq/xs first
+    uint32_t *bnd;           // stripe boundary rows, bnd_words per block (multi-stripe bins)
+    int64_t bnd_words;
+    int32_t *exact_list;     // i16-pass pairs near 32767: re-run in 32-bit arithmetic
+    int32_t *exact_count;
+    int exact_threshold;
     int8_t mat[625];
     int8_t xq[128], xs[128]; // byte -> matrix index (internal alphabet inputs)
 };
@@ -101,10 +109,10 @@ __device__ __forceinline__ uint64_t best_key(int v, int col, int row) {
 
 template <int R>
 __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
-                                         uint32_t *profA, uint32_t *profB) {
+                                         uint32_t *profA, uint32_t *profB, int stripes,
+                                         uint32_t *bnd) {
     constexpr int W = words_for(R);
     const int lane = threadIdx.x & 31;
-    const int i0 = lane * R;
 
     const int qlA = a.qlen[pA];
     const int slA = a.slen[pA];
@@ -115,6 +123,22 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     const int8_t *qB = pB >= 0 ? a.q + a.qoff[pB] : qA;
     const int8_t *sB = pB >= 0 ? a.s + a.soff[pB] : sA;
     const int N = max(slA, slB);
+    const int segA = max(1, (qlA + a.ssw_lanes - 1) / a.ssw_lanes);
+    const int segB = max(1, (qlB + a.ssw_lanes - 1) / a.ssw_lanes);
+    const uint32_t NGO = pack2(-a.gap_open, -a.gap_open);
+    const uint32_t NGE = pack2(-a.gap_extend, -a.gap_extend);
+    const uint32_t NEGINF = 0x80008000u;
+    // sign-extend byte r%4 of the A word into the low half, of the B word
+    // into the high half
+    constexpr uint32_t SEL[4] = {0xC480u, 0xD591u, 0xE6A2u, 0xF7B3u};
+    uint64_t kA = 0, kB = 0;
+
+    // Queries longer than one stripe (32 lanes x R rows) run stripe after
+    // stripe; the last row of a stripe (H, F, Fm per column) goes to `bnd`
+    // and enters the next stripe at lane 0.  Lane 0 reads column k at step k
+    // and lane 31 writes column k-31 at step k, so one buffer serves as both.
+    for (int st = 0; st < stripes; ++st) {
+    const int i0 = (st * 32 + lane) * R;
 
     // ---- profile of this lane's rows for all 26 letters (25 + pad column)
     int qa[R], qb[R];
@@ -151,8 +175,6 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     __syncwarp();
 
     // ---- SSW lane starts of this lane's rows -> per-row clear masks for Fm
-    const int segA = max(1, (qlA + a.ssw_lanes - 1) / a.ssw_lanes);
-    const int segB = max(1, (qlB + a.ssw_lanes - 1) / a.ssw_lanes);
     uint32_t mask[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -161,13 +183,6 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
         if ((i0 + r) % segB == 0) m &= 0x0000FFFFu;
         mask[r] = m;
     }
-
-    const uint32_t NGO = pack2(-a.gap_open, -a.gap_open);
-    const uint32_t NGE = pack2(-a.gap_extend, -a.gap_extend);
-    const uint32_t NEGINF = 0x80008000u;
-    // sign-extend byte r%4 of the A word into the low half, of the B word
-    // into the high half
-    constexpr uint32_t SEL[4] = {0xC480u, 0xD591u, 0xE6A2u, 0xF7B3u};
 
     uint32_t E[R], H[R];
 #pragma unroll
@@ -186,7 +201,12 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
         uint32_t inFm = __shfl_up_sync(0xFFFFFFFFu, outFm, 1);
         uint32_t inLet = __shfl_up_sync(0xFFFFFFFFu, outLet, 1);
         if (lane == 0) {
-            inH = 0u; inF = 0u; inFm = 0u;
+            if (st == 0 || k >= N) {
+                inH = 0u; inF = 0u; inFm = 0u;
+            } else {
+                const uint32_t *b = bnd + 3 * (size_t)k;
+                inH = b[0]; inF = b[1]; inFm = b[2];
+            }
             // the subject letters of column k enter at lane 0 (an L1-resident
             // byte load; cheaper here than a shuffle-fed prefetch window)
             int la = k < slA ? sA[k] : kPadLetter;
@@ -224,6 +244,10 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             outF = F;
             outFm = Fm;
             outLet = inLet;
+            if (lane == 31 && st + 1 < stripes) {
+                uint32_t *b = bnd + 3 * (size_t)j;
+                b[0] = outH; b[1] = outF; b[2] = outFm;
+            }
             const uint32_t nm = __vimax_s16x2_relu(runmax, cm);
             if (nm != runmax) {
                 // the lane's running max rose in this column: remember the
@@ -248,9 +272,12 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
         diag = inH;
     }
 
+    kA = max(kA, best_key(lo16(runmax), colA, rowA));
+    kB = max(kB, best_key(hi16(runmax), colB, rowB));
+    __syncwarp();
+    }   // stripes
+
     // ---- warp reduction: max value, then first column, then smallest row
-    uint64_t kA = best_key(lo16(runmax), colA, rowA);
-    uint64_t kB = best_key(hi16(runmax), colB, rowB);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         kA = max(kA, __shfl_xor_sync(0xFFFFFFFFu, kA, o));
@@ -267,6 +294,10 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
                 // u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
                 const int slot = atomicAdd(a.rerun_count, 1);
                 a.rerun[slot] = p;
+            } else if (a.ssw_lanes == 8 && a.exact_list && v >= a.exact_threshold) {
+                // near the i16 limit: 16-bit lanes may wrap, redo in 32 bits
+                const int slot = atomicAdd(a.exact_count, 1);
+                a.exact_list[slot] = p;
             } else {
                 a.score[p] = v;
                 a.ref_end[p] = col;
@@ -278,13 +309,13 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
 }
 
 template <int R>
-__global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args a) {
+__global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args a, int bin,
+                                                    int stripes) {
     extern __shared__ __align__(16) uint8_t smem[];
     int8_t *smat = reinterpret_cast<int8_t *>(smem);
     uint32_t *profA = reinterpret_cast<uint32_t *>(smem + kSmatBytes);
     uint32_t *profB = profA + profile_bytes(R) / 4;
     const int lane = threadIdx.x;
-    const int bin = R - 1;
     const int start = a.rinfo[2 * bin];
     const int count = a.rinfo[2 * bin + 1];
     const int ntask = (count + 1) / 2;
@@ -302,14 +333,16 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
         if (t >= ntask) break;
         const int pA = a.sorted[start + 2 * t];
         const int pB = 2 * t + 1 < count ? a.sorted[start + 2 * t + 1] : -1;
-        run_task<R>(a, pA, pB, smat, profA, profB);
+        run_task<R>(a, pA, pB, smat, profA, profB, stripes,
+                    a.bnd ? a.bnd + (size_t)blockIdx.x * a.bnd_words : nullptr);
     }
 }
 
 // ---------------------------------------------------------------- binning
 
 __device__ __forceinline__ int pair_bin(int ql, int sl) {
-    const int rb = (ql + 31) / 32 - 1;                  // 0..31
+    const int rb = ql <= kStripeRows ? (ql + 31) / 32 - 1                 // 0..31
+                                     : 30 + (ql + kStripeRows - 1) / kStripeRows;  // 32..38
     const int sb = min(sl >> 5, kSBins - 1);
     return rb * kSBins + (kSBins - 1 - sb);             // long subjects first
 }
@@ -317,17 +350,18 @@ __device__ __forceinline__ int pair_bin(int ql, int sl) {
 // list == nullptr: pairs 0..n-1; else list[0 .. *list_n)
 __global__ void bin_count_kernel(int64_t n, const int32_t *list, const int32_t *list_n,
                                  const int32_t *qlen, const int32_t *slen, int32_t *counts,
-                                 int32_t *status) {
+                                 int32_t *status, int max_qlen, int32_t *multi_maxn) {
     const int64_t limit = list ? (int64_t)*list_n : n;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int p = list ? list[i] : (int)i;
         const int ql = qlen[p], sl = slen[p];
-        if (ql < 1 || ql > TPZ_SW_MAX_QLEN || sl < 0 || sl >= TPZ_SW_MAX_SLEN) {
+        if (ql < 1 || ql > max_qlen || sl < 0 || sl >= TPZ_SW_MAX_SLEN) {
             status[p] = TPZ_SW_INVALID;
             continue;
         }
         atomicAdd(&counts[pair_bin(ql, sl)], 1);
+        if (ql > kStripeRows && multi_maxn) atomicMax(multi_maxn, sl);
     }
 }
 
@@ -366,13 +400,13 @@ __global__ void bin_scan_kernel(const int32_t *counts, int32_t *cursor, int32_t 
 
 __global__ void bin_scatter_kernel(int64_t n, const int32_t *list, const int32_t *list_n,
                                    const int32_t *qlen, const int32_t *slen, int32_t *cursor,
-                                   int32_t *sorted) {
+                                   int32_t *sorted, int max_qlen) {
     const int64_t limit = list ? (int64_t)*list_n : n;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int p = list ? list[i] : (int)i;
         const int ql = qlen[p], sl = slen[p];
-        if (ql < 1 || ql > TPZ_SW_MAX_QLEN || sl < 0 || sl >= TPZ_SW_MAX_SLEN) continue;
+        if (ql < 1 || ql > max_qlen || sl < 0 || sl >= TPZ_SW_MAX_SLEN) continue;
         const int pos = atomicAdd(&cursor[pair_bin(ql, sl)], 1);
         sorted[pos] = p;
     }
@@ -401,7 +435,7 @@ __global__ void __launch_bounds__(256) dpx_probe_kernel(int iters, uint32_t inc,
 
 // ------------------------------------------------------------ host driver
 
-typedef void (*KernelFn)(const Args);
+typedef void (*KernelFn)(const Args, int, int);
 
 template <int R>
 struct Table {
@@ -463,27 +497,49 @@ static int launch_cfg(const LaunchCfg **out) {
 
 static thread_local int64_t g_last_launches = 0;
 
+// R and stripe count of a row bin
+__host__ __device__ constexpr int bin_rows(int b) { return b < kMaxR ? b + 1 : kMaxR; }
+__host__ __device__ constexpr int bin_stripes(int b) { return b < kMaxR ? 1 : b - 30; }
+constexpr int kUsedRBins = kMaxR + kMaxStripes - 1;     // 39
+
 static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t *list,
                         const int32_t *list_n, int32_t *counts, int32_t *cursor, int32_t *sorted,
-                        cudaStream_t st, int64_t &launches) {
+                        int32_t *multi_maxn, cudaStream_t st, int64_t &launches,
+                        int *host_maxn) {
     const int nsm = sm_count();
     TPZ_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * kBins, st));
     const int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
     bin_count_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, counts,
-                                                      a.status);
+                                                      a.status, TPZ_SW_MAX_QLEN, multi_maxn);
     bin_scan_kernel<<<1, 1024, 0, st>>>(counts, cursor, const_cast<int32_t *>(a.rinfo),
                                         a.next_task);
     bin_scatter_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, cursor,
-                                                        sorted);
+                                                        sorted, TPZ_SW_MAX_QLEN);
     launches += 4;
+    if (host_maxn) {
+        // the boundary buffer of multi-stripe bins is sized by the longest
+        // subject among queries longer than one stripe
+        TPZ_CUDA(cudaMemcpyAsync(host_maxn, multi_maxn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        TPZ_CUDA(cudaStreamSynchronize(st));
+        if (*host_maxn > 0) {
+            a.bnd_words = 3 * ((int64_t)*host_maxn + 1);
+            const size_t bytes = sizeof(uint32_t) * (size_t)a.bnd_words * nsm *
+                                 cfg->blocks_per_sm[kMaxR - 1];
+            TPZ_CUDA(cudaMallocAsync((void **)&a.bnd, bytes, st));
+        }
+    }
     // one persistent kernel per row bin, longest rows first, spread over the
-    // auxiliary streams so that each kernel's tail overlaps the next one
+    // auxiliary streams so that each kernel's tail overlaps the next one;
+    // the multi-stripe bins share one boundary buffer and stay on aux[0]
     TPZ_CUDA(cudaEventRecord(cfg->fork, st));
     for (int i = 0; i < kAuxStreams; ++i) TPZ_CUDA(cudaStreamWaitEvent(cfg->aux[i], cfg->fork, 0));
-    for (int r = kMaxR; r >= 1; --r) {
-        const int grid = nsm * cfg->blocks_per_sm[r - 1];
-        cudaStream_t xs = cfg->aux[(kMaxR - r) % kAuxStreams];
-        cfg->fn[r - 1]<<<grid, 32, cfg->smem[r - 1], xs>>>(a);
+    int rr = 0;
+    for (int b = kUsedRBins - 1; b >= 0; --b) {
+        const int R = bin_rows(b), S = bin_stripes(b);
+        if (S > 1 && !a.bnd) continue;
+        const int grid = nsm * cfg->blocks_per_sm[R - 1];
+        cudaStream_t xs = S > 1 ? cfg->aux[0] : cfg->aux[rr++ % kAuxStreams];
+        cfg->fn[R - 1]<<<grid, 32, cfg->smem[R - 1], xs>>>(a, b, S);
         ++launches;
     }
     for (int i = 0; i < kAuxStreams; ++i) {
@@ -494,12 +550,62 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
     return TPZ_OK;
 }
 
+// 32-bit re-run of i16-pass pairs whose maximum came near 32767 (16-bit
+// lanes could wrap there): the same recurrence with the i16 lane length,
+// one thread per pair, rows and columns in a plain loop.  Only pairs whose
+// score can pass 32767 - 2*max(M) get here -- query and subject both longer
+// than ~1900 residues of near-identity.
+constexpr int kExactThreads = 128;
+
+__global__ void __launch_bounds__(kExactThreads) sw_exact_kernel(const __grid_constant__ Args a,
+                                                                 int32_t *scratch) {
+    const int n = *a.exact_count;
+    int32_t *E = scratch + (size_t)threadIdx.x * 2 * TPZ_SW_MAX_QLEN;
+    int32_t *Hc = E + TPZ_SW_MAX_QLEN;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int p = a.exact_list[i];
+        const int ql = a.qlen[p], sl = a.slen[p];
+        const int8_t *qp = a.q + a.qoff[p];
+        const int8_t *sp = a.s + a.soff[p];
+        const int seg = max(1, (ql + 7) / 8);
+        for (int r = 0; r < ql; ++r) { E[r] = 0; Hc[r] = 0; }
+        int best = 0, bc = -1, br = 0;
+        for (int c = 0; c < sl; ++c) {
+            int sc = sp[c];
+            if (a.translate) sc = a.xs[sc & 127];
+            const int8_t *mrow = a.mat + 25 * sc;
+            int F = 0, Fm = 0, D = 0;
+            for (int r = 0; r < ql; ++r) {
+                if (r % seg == 0) Fm = 0;
+                int qc = qp[r];
+                if (a.translate) qc = a.xq[qc & 127];
+                const int X = max(max(0, D + mrow[qc]), E[r]);
+                const int h = max(X, F);
+                const int Xg = X - a.gap_open;
+                const int Gp = max(Fm - a.gap_open, Xg);
+                E[r] = max(E[r] - a.gap_extend, Gp);
+                F = max(F - a.gap_extend, Xg);
+                Fm = max(Fm - a.gap_extend, Xg);
+                D = Hc[r];
+                Hc[r] = h;
+                if (h > best) { best = h; bc = c; br = r; }
+            }
+        }
+        if (best >= 32767) {
+            a.score[p] = 32767; a.ref_end[p] = -1; a.read_end[p] = -1; a.status[p] = TPZ_SW_DROPPED;
+        } else {
+            a.score[p] = best; a.ref_end[p] = bc; a.read_end[p] = best > 0 ? br : 0;
+            a.status[p] = TPZ_SW_OK;
+        }
+    }
+}
+
 int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs) {
     g_last_launches = 0;
-    if (n < 0 || n > INT32_MAX / 2 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
+    if (n < 0 || n > INT32_MAX / 3 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
     if (!(go > ge && ge >= 0 && go <= 255)) {
         set_error("tpz_sw_batch: requires 255 >= gap_open > gap_extend >= 0");
         return TPZ_E_ARG;
@@ -513,9 +619,10 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     int rc = launch_cfg(&cfg);
     if (rc) return rc;
 
-    // workspace: counts, cursor, rinfo, next_task, rerun_count | sorted, rerun
-    const size_t small = sizeof(int32_t) * (2 * kBins + 2 * kRBins + kRBins + 4);
-    const size_t bytes = small + sizeof(int32_t) * 2 * (size_t)n;
+    // workspace: counts, cursor, rinfo, next_task, rerun_count, multi_maxn,
+    // exact_count | sorted, rerun, exact_list
+    const size_t small = sizeof(int32_t) * (2 * kBins + 2 * kRBins + kRBins + 8);
+    const size_t bytes = small + sizeof(int32_t) * 3 * (size_t)n;
     char *ws = nullptr;
     TPZ_CUDA(cudaMallocAsync((void **)&ws, bytes, st));
     int32_t *counts = (int32_t *)ws;
@@ -523,8 +630,11 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     int32_t *rinfo = cursor + kBins;
     int32_t *next_task = rinfo + 2 * kRBins;
     int32_t *rerun_count = next_task + kRBins;
+    int32_t *multi_maxn = rerun_count + 1;
+    int32_t *exact_count = rerun_count + 2;
     int32_t *sorted = (int32_t *)(ws + small);
     int32_t *rerun = sorted + n;
+    int32_t *exact_list = rerun + n;
 
     Args a;
     a.q = q; a.qoff = qoff; a.qlen = qlen; a.s = s; a.soff = soff; a.slen = slen;
@@ -532,8 +642,8 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     a.sorted = sorted; a.rinfo = rinfo; a.next_task = next_task;
     a.rerun = rerun; a.rerun_count = rerun_count;
     a.gap_open = go; a.gap_extend = ge;
-    int mn = 0;
-    for (int i = 0; i < 625; ++i) mn = std::min<int>(mn, mat[i]);
+    int mn = 0, mx = 0;
+    for (int i = 0; i < 625; ++i) { mn = std::min<int>(mn, mat[i]); mx = std::max<int>(mx, mat[i]); }
     a.bias = -mn;
     memcpy(a.mat, mat, 625);
     a.translate = (xq && xs) ? 1 : 0;
@@ -543,16 +653,38 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
         memcpy(a.xq, xq, 128);
         memcpy(a.xs, xs, 128);
     }
+    a.bnd = nullptr;
+    a.bnd_words = 0;
+    a.exact_list = exact_list;
+    a.exact_count = exact_count;
+    a.exact_threshold = 32767 - 2 * std::max(mx, 1);
 
     int64_t launches = 0;
-    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, sizeof(int32_t), st));
+    int host_maxn = 0;
+    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, 3 * sizeof(int32_t), st));
     a.ssw_lanes = 16;
-    rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, st, launches);
-    if (rc) { cudaFreeAsync(ws, st); return rc; }
+    rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, multi_maxn, st,
+                      launches, &host_maxn);
+    if (rc) { if (a.bnd) cudaFreeAsync(a.bnd, st); cudaFreeAsync(ws, st); return rc; }
     a.ssw_lanes = 8;
-    rc = launch_round(cfg, a, n, rerun, rerun_count, counts, cursor, sorted, st, launches);
+    rc = launch_round(cfg, a, n, rerun, rerun_count, counts, cursor, sorted, multi_maxn, st,
+                      launches, nullptr);
+    if (rc == TPZ_OK && host_maxn > 0) {
+        // only queries longer than one stripe can come near 32767
+        int32_t *scratch = nullptr;
+        rc = cudaMallocAsync((void **)&scratch,
+                             sizeof(int32_t) * 2 * (size_t)TPZ_SW_MAX_QLEN * kExactThreads, st)
+                 == cudaSuccess ? TPZ_OK : cuda_fail(cudaGetLastError(), "exact scratch");
+        if (rc == TPZ_OK) {
+            sw_exact_kernel<<<1, kExactThreads, 0, st>>>(a, scratch);
+            ++launches;
+            cudaFreeAsync(scratch, st);
+        }
+    }
+    if (a.bnd) cudaFreeAsync(a.bnd, st);
     if (rc) { cudaFreeAsync(ws, st); return rc; }
     TPZ_CUDA(cudaFreeAsync(ws, st));
+    TPZ_CUDA(cudaGetLastError());
     g_last_launches = launches;
     return TPZ_OK;
 }
@@ -696,6 +828,7 @@ namespace tpz {
 namespace sw {
 
 constexpr int64_t kNoAllocMaxPairs = TPZ_SW_NOALLOC_MAX_PAIRS;
+constexpr int kNoAllocMaxQlen = TPZ_SW_NOALLOC_MAX_QLEN;   // one stripe
 constexpr size_t kNoAllocWords = 2 * (size_t)kBins + 2 * kRBins + kRBins + 4 + 2 * (size_t)kNoAllocMaxPairs;
 
 // One copy per device that loads the library, kept until the process exits.
@@ -752,12 +885,12 @@ static int noalloc_round(const NoAllocDev *d, Args &a, int64_t n, const int32_t 
     TPZ_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * kBins, st));
     const int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
     bin_count_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, counts,
-                                                      a.status);
+                                                      a.status, kNoAllocMaxQlen, nullptr);
     bin_scan_kernel<<<1, 1024, 0, st>>>(counts, cursor, const_cast<int32_t *>(a.rinfo), a.next_task);
     bin_scatter_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, cursor,
-                                                        sorted);
+                                                        sorted, kNoAllocMaxQlen);
     for (int r = kMaxR; r >= 1; --r)
-        d->fn[r - 1]<<<nsm * d->blocks_per_sm[r - 1], 32, smem_bytes(r), st>>>(a);
+        d->fn[r - 1]<<<nsm * d->blocks_per_sm[r - 1], 32, smem_bytes(r), st>>>(a, r - 1, 1);
     TPZ_CUDA(cudaGetLastError());
     return TPZ_OK;
 }
@@ -819,6 +952,11 @@ extern "C" int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int
     a.translate = 0;
     memset(a.xq, 0, sizeof a.xq);
     memset(a.xs, 0, sizeof a.xs);
+    a.bnd = nullptr;
+    a.bnd_words = 0;
+    a.exact_list = nullptr;
+    a.exact_count = nullptr;
+    a.exact_threshold = 32767;
 
     // the rerun counter carries the previous call's value: clear it
     TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, sizeof(int32_t), st));
