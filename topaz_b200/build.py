@@ -19,6 +19,15 @@ LIB = os.path.join(LIBDIR, "libtopaz_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["tpz_common.cu", "sw_kernel.cu", "search_kernels.cu", "search_host.cu"]
+HOSTDIR = os.path.join(HERE, "host")
+HOST_SOURCES = ["tpzh_fasta.c", "tpzh_seg.c", "tpzh_sais.c", "tpzh_index.c", "tpzh_stats.c",
+                "tpzh_search.c", "tpzh_main.c"]
+CLI = os.path.join(LIBDIR, "topaz")
+CC = os.environ.get("CC", "gcc")
+# plain IEEE double arithmetic in the host code (no fast-math, no FMA
+# contraction) so that SEG and E-values round exactly as the reference does
+HOST_CFLAGS = ["-O2", "-g", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result",
+               "-fvisibility=hidden", "-ffp-contract=off"]
 
 
 def sources():
@@ -36,8 +45,9 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)
                         if f.endswith((".cuh", ".h", ".inc"))]
+    deps += [os.path.join(HOSTDIR, f) for f in os.listdir(HOSTDIR) if f.endswith((".c", ".h"))]
     deps.append(os.path.join(ROOT, "include", "topaz_b200.h"))
-    if not force and not _stale(LIB, deps):
+    if not force and not _stale(LIB, deps) and not _stale(CLI, deps):
         return LIB
     objs = []
     procs = []
@@ -50,6 +60,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))
         objs.append(obj)
+    for src in HOST_SOURCES:
+        obj = os.path.join(LIBDIR, src + ".o")
+        cmd = [CC, *HOST_CFLAGS, "-I", os.path.join(ROOT, "include"), "-c",
+               os.path.join(HOSTDIR, src), "-o", obj]
+        procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))
+        objs.append(obj)
     failed = False
     for p, src in procs:
         out, _ = p.communicate()
@@ -60,8 +76,11 @@ def build(verbose: bool = False, force: bool = False) -> str:
             sys.stderr.write("nvcc failed on %s\n" % src)
     if failed:
         raise RuntimeError("building libtopaz_b200.so failed")
-    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xlinker", "-Bsymbolic"]
+    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xlinker", "-Bsymbolic", "-lm"]
     subprocess.check_call(link)
+    cli = [CC, "-O2", "-o", CLI, os.path.join(HOSTDIR, "tpzh_cli.c"), "-I", HOSTDIR, "-L", LIBDIR,
+           "-ltopaz_b200", "-Wl,-rpath,$ORIGIN", "-lm"]
+    subprocess.check_call(cli)
     return LIB
 
 

@@ -1,0 +1,276 @@
+/*
+ * tpzh_search.c -- `topaz search` on the B200: the host part of
+ * search_alloc/search_pthread (src/engine.c:38-87, :493-559) around the
+ * device batch entry point tpz_search_batch.
+ *
+ * Per query, as the reference does it (src/engine.c:193-248,
+ * src/ssw_wrapper.c:157-245, src/utils.c:140-152): every hit that was
+ * aligned (SW score, or gapless score < 40 with bitscore 0 and E-value
+ * 1000) in hitlist traversal order, stably sorted by bitscore descending,
+ * the first -H of them, printed when the E-value is <= -E.  Bitscores and
+ * E-values come from tpz_karlin (the C library's log/exp, same expression
+ * order).  Queries print in input order; the reference prints them in
+ * completion order of its threads, so parity is per-query block.
+ */
+#define _GNU_SOURCE
+#include "tpzh.h"
+#include "../../include/topaz_b200.h"
+
+#include <errno.h>
+#include <fcntl.h>
+#include <inttypes.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <sys/time.h>
+#include <unistd.h>
+
+void tpzh_options_defaults(tpzh_options *o) {
+    memset(o, 0, sizeof *o);
+    o->num_threads = 1;
+    o->num_hits = 100;
+    o->evalue = 1e-3;
+    o->gap_open = 11;
+    o->gap_extend = 1;
+    o->lambda = 0.267;
+    o->k = 0.041;
+    o->H = 0.140;
+    o->matrix = "BLOSUM62";
+    o->min_hit_length = 5;
+    o->min_hit_score = 1;
+    o->number_of_seeds = 300000;
+    o->number_of_alignments = 5000;
+    o->superfast = 1;
+    o->seg_enabled = 1;
+    o->batch = 2000;
+}
+
+typedef struct {
+    const char *data;
+    uint64_t size;
+} map_t;
+
+static int map_file(const char *prefix, const char *ext, map_t *m) {
+    char name[4096];
+    snprintf(name, sizeof name, "%s%s", prefix, ext);
+    const int fd = open(name, O_RDONLY);
+    struct stat sb;
+    if (fd < 0 || fstat(fd, &sb) != 0) return -1;
+    m->size = (uint64_t)sb.st_size;
+    m->data = m->size ? mmap(NULL, m->size, PROT_READ, MAP_PRIVATE, fd, 0) : NULL;
+    close(fd);
+    if (m->size && m->data == MAP_FAILED) return -1;
+    return 0;
+}
+
+typedef struct {
+    int64_t idx;
+    double bits, evalue;
+} ranked_t;
+
+/* stable by construction: insertion order breaks ties (glibc qsort is a
+ * merge sort here, so equal bitscores keep traversal order) */
+static void stable_sort_bits(ranked_t *v, int64_t n, ranked_t *tmp) {
+    for (int64_t w = 1; w < n; w *= 2) {
+        for (int64_t lo = 0; lo < n; lo += 2 * w) {
+            int64_t mid = lo + w < n ? lo + w : n, hi = lo + 2 * w < n ? lo + 2 * w : n;
+            int64_t a = lo, b = mid, k = lo;
+            while (a < mid && b < hi) tmp[k++] = (v[b].bits > v[a].bits) ? v[b++] : v[a++];
+            while (a < mid) tmp[k++] = v[a++];
+            while (b < hi) tmp[k++] = v[b++];
+        }
+        memcpy(v, tmp, sizeof(ranked_t) * n);
+    }
+}
+
+static int8_t g_int2idx[128];
+
+static void init_int2idx(void) {
+    static const char order[] = "ACMLJIVTSKRQZEDBNHYFWXP*G";
+    static const char mat[] = "ARNDCQEGHILKMFPSTWYVBJZX*";
+    for (int i = 0; i < 128; ++i) g_int2idx[i] = 23;
+    for (int i = 0; i < 25; ++i) g_int2idx['A' + i] = (int8_t)(strchr(mat, order[i]) - mat);
+}
+
+typedef struct {
+    char *id;
+    int id_len;
+    char *seq;      /* internal alphabet */
+    int len;
+} query_t;
+
+int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
+    struct timeval t0, t1;
+    gettimeofday(&t0, NULL);
+    map_t T, SA, phr, ind;
+    if (map_file(prefix, ".psq", &T) || map_file(prefix, ".SA", &SA) || map_file(prefix, ".phr", &phr)) {
+        fprintf(stderr, "Error: could not load database, %s\n", strerror(errno));
+        return -1;
+    }
+    fprintf(stderr, "read T (%s.psq), file size is %" PRIu64 " bytes\n", prefix, T.size);
+    fprintf(stderr, "read SA (%s.SA), file size is %" PRIu64 " bytes\n", prefix, SA.size);
+    if (SA.size != T.size * 8) {
+        fprintf(stderr, "Error: SA (%s.SA, %" PRIu64 " bytes) should be 8 x T (%s.psq, %" PRIu64 " bytes)!\nExiting...\n",
+                prefix, SA.size, prefix, T.size);
+        exit(EXIT_FAILURE);
+    }
+    uint64_t Psize = 0;
+    for (uint64_t i = 0; i < phr.size; ++i) {
+        if (phr.data[i] == '\0') break;
+        if (phr.data[i] == '\n') Psize++;
+    }
+    fprintf(stderr, "read protein headers (%s.phr), file size is %" PRIu64 " bytes\n", prefix, phr.size);
+    fprintf(stderr, "%" PRIu64 " proteins in database\n", Psize);
+    if (map_file(prefix, ".ind", &ind)) {
+        fprintf(stderr, "Error: could not open %s.ind, %s\n", prefix, strerror(errno));
+        return -1;
+    }
+    if (ind.size != Psize * 24) {
+        fprintf(stderr, "Error: index is the wrong size (read %" PRIu64 ", expected %" PRIu64 ")", ind.size, Psize * 24);
+        exit(EXIT_FAILURE);
+    }
+    const uint64_t db_size = T.size - Psize, db_proteins = Psize;
+    fprintf(stderr, "db size = %" PRIu64 "\n", db_size);
+    fprintf(stderr, "db proteins = %" PRIu64 "\n", db_proteins);
+
+    int8_t mat[625];
+    if (tpz_matrix(o->matrix, mat) != 0) {
+        fprintf(stderr, "Error: %s\n", tpz_last_error());
+        return -1;
+    }
+    tpz_index *ix = NULL;
+    if (tpz_index_create((const uint8_t *)T.data, (int64_t)T.size, (const int64_t *)SA.data, ind.data,
+                         (int64_t)Psize, &ix) != 0) {
+        fprintf(stderr, "Error: %s\n", tpz_last_error());
+        return -1;
+    }
+    typedef struct { uint64_t hs, ps; int32_t hl, pl; } rec_t;
+    const rec_t *recs = (const rec_t *)ind.data;
+    init_int2idx();
+
+    if (o->superfast) printf("qseqid sseqid evalue bitscore\n");
+    else printf("qseqid sseqid pident length mismatch gapopen qstart qend sstart send evalue bitscore\n");
+
+    tpzh_fasta f;
+    if (tpzh_fasta_open(&f, fasta) != 0) exit(EXIT_FAILURE);
+    const int64_t B = o->batch > 0 ? o->batch : 2000;
+    query_t *qs = calloc(B, sizeof(query_t));
+    uint64_t nonzero = 0, total_hits = 0;
+    int done = 0;
+    tpz_search_opts so;
+    memset(&so, 0, sizeof so);
+    so.num_hits = o->num_hits;
+    so.gap_open = o->gap_open;
+    so.gap_extend = o->gap_extend;
+    so.min_hit_length = o->min_hit_length;
+    so.seeds = o->number_of_seeds;
+    so.alignments = o->number_of_alignments;
+    so.mat625 = mat;
+    while (!done) {
+        int64_t nq = 0;
+        tpzh_record r;
+        while (nq < B) {
+            const int rc = tpzh_fasta_next(&f, &r);
+            if (rc < 0) exit(EXIT_FAILURE);
+            if (rc == 0) { done = 1; break; }
+            if (o->seg_enabled) tpzh_seg_mask(r.seq, r.seq_len);
+            for (int i = 0; i < r.seq_len; ++i) r.seq[i] = tpzh_aa2internal(r.seq[i]);
+            qs[nq].id = r.id; qs[nq].id_len = r.id_len;
+            qs[nq].seq = r.seq; qs[nq].len = r.seq_len;
+            nq++;
+        }
+        if (nq == 0) break;
+        int64_t total = 0;
+        int64_t *qoff = malloc(sizeof(int64_t) * nq);
+        int32_t *qlen = malloc(sizeof(int32_t) * nq);
+        for (int64_t i = 0; i < nq; ++i) { qoff[i] = total; qlen[i] = qs[i].len; total += qs[i].len; }
+        char *cat = malloc(total + 1);
+        for (int64_t i = 0; i < nq; ++i) memcpy(cat + qoff[i], qs[i].seq, qs[i].len);
+        tpz_search_result *res = NULL;
+        if (tpz_search_batch(ix, cat, qoff, qlen, nq, &so, &res) != 0) {
+            fprintf(stderr, "Error: %s\n", tpz_last_error());
+            exit(EXIT_FAILURE);
+        }
+        int64_t maxh = 1;
+        for (int64_t q = 0; q < nq; ++q) {
+            const int64_t nh = res->hit_off[q + 1] - res->hit_off[q];
+            if (nh > maxh) maxh = nh;
+        }
+        ranked_t *rk = malloc(sizeof(ranked_t) * maxh), *tmp = malloc(sizeof(ranked_t) * maxh);
+        for (int64_t q = 0; q < nq; ++q) {
+            if (res->status[q] & TPZ_Q_SA_END)
+                fprintf(stderr, "Warning: %.*s reached the end of the suffix array (the reference reads past its mapping there)\n",
+                        qs[q].id_len, qs[q].id);
+            const int64_t a = res->hit_off[q], b = res->hit_off[q + 1];
+            int64_t n = 0;
+            for (int64_t h = a; h < b; ++h) {
+                const int st = res->sw_status[h];
+                if (st == TPZ_SW_OK) {
+                    rk[n].idx = h;
+                    tpz_karlin(qs[q].len, db_size, db_proteins, o->lambda, o->k, o->H, res->rawscore[h],
+                               &rk[n].bits, &rk[n].evalue);
+                    n++;
+                } else if (st == TPZ_SW_GAPLESS_LOW) {
+                    rk[n].idx = h; rk[n].bits = 0; rk[n].evalue = 1000; n++;
+                }
+            }
+            stable_sort_bits(rk, n, tmp);
+            if (n > o->num_hits) n = o->num_hits;
+            int count = 0;
+            int8_t *qidx = NULL;
+            for (int64_t i = 0; i < n; ++i) {
+                if (!(rk[i].evalue <= o->evalue)) continue;
+                const int64_t h = rk[i].idx;
+                const rec_t *pr = &recs[res->protein[h]];
+                const char *sid;
+                const int sl = tpzh_header_id(phr.data + pr->hs, pr->hl, &sid);
+                if (o->superfast) {
+                    printf("%.*s\t%.*s\t%.3e\t%d\n", qs[q].id_len, qs[q].id, sl, sid, rk[i].evalue,
+                           (int)rk[i].bits);
+                } else {
+                    tpzh_stats stt;
+                    memset(&stt, 0, sizeof stt);
+                    if (res->sw_status[h] == TPZ_SW_OK) {
+                        if (!qidx) {
+                            qidx = malloc(qs[q].len + 1);
+                            for (int j = 0; j < qs[q].len; ++j) qidx[j] = g_int2idx[(int)qs[q].seq[j] & 127];
+                        }
+                        int8_t *sidx = malloc(pr->pl + 1);
+                        for (int j = 0; j < pr->pl; ++j) sidx[j] = g_int2idx[(int)T.data[pr->ps + j] & 127];
+                        tpzh_align_stats(qidx, qs[q].len, sidx, pr->pl, mat, o->gap_open, o->gap_extend,
+                                         res->qend[h], res->send[h], res->rawscore[h], &stt);
+                        free(sidx);
+                    } else {
+                        stt.qstart = stt.sstart = -1;
+                        stt.length = stt.mismatch = stt.gapopen = -1;
+                        stt.identity = INFINITY;
+                    }
+                    printf("%.*s\t%.*s\t%.2f\t%d\t%d\t%d\t%d\t%d\t%d\t%d\t%.3e\t%d\n", qs[q].id_len, qs[q].id,
+                           sl, sid, stt.identity * 100, stt.length, stt.mismatch, stt.gapopen,
+                           stt.qstart + 1, res->qend[h] + 1, stt.sstart + 1, res->send[h] + 1,
+                           rk[i].evalue, (int)rk[i].bits);
+                }
+                ++count;
+            }
+            free(qidx);
+            if (count) { nonzero++; total_hits += count; }
+        }
+        free(rk); free(tmp);
+        tpz_search_result_free(res);
+        free(cat); free(qoff); free(qlen);
+        for (int64_t i = 0; i < nq; ++i) { free(qs[i].id); free(qs[i].seq); }
+    }
+    fflush(stdout);
+    tpzh_fasta_close(&f);
+    free(qs);
+    tpz_index_destroy(ix);
+    gettimeofday(&t1, NULL);
+    fprintf(stderr, "output %" PRIu64 " hits for %" PRIu64 " queries\n", total_hits, nonzero);
+    fprintf(stderr, "elapsed time: %.1f seconds\n",
+            ((t1.tv_sec - t0.tv_sec) * 1000.0 + (t1.tv_usec - t0.tv_usec) / 1000.0) / 1000);
+    fprintf(stderr, "done!\n");
+    return 0;
+}
