@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--search-batch", type=int, default=5000,
+                    help="queries per tpz_search_batch call in the full-search section")
+    ap.add_argument("--no-search", action="store_true",
+                    help="skip the full-search (config 2) section")
     return ap.parse_args()
 
 
@@ -138,6 +142,97 @@ def read_traffic():
     except OSError:
         pass
     return None
+
+
+SEARCH_WORKLOAD = ("full search, mid size: 1,000,000-protein synthetic DB (log-normal lengths "
+                   "median 300, 50-2000; ~359M residues, int64 SA ~2.9 GB resident in HBM), "
+                   "10,000 queries of 50-1500 residues (half mutated from DB proteins at 30-90%% "
+                   "identity with indels, half random), SEG on, BLOSUM62 11/1, -H 100 -E 1e-3, "
+                   "batches of %d queries")
+
+
+def search_bench(args, dev):
+    """Full-search throughput (queries/s) through tpz_search_batch with host
+    buffers (SEG + internal alphabet on the host, H2D of queries, D2H of
+    hit lists inside the timed region), with the reference binary timed on a
+    query sample on all host threads and its output compared per query."""
+    import subprocess
+    import tempfile
+
+    import torch
+
+    import oracle
+    from topaz_b200 import build as B, dbformat, gpu_sa, native, synth
+
+    t0 = time.perf_counter()
+    res, lens = synth.protein_db_arrays(1_000_000, seed=args.seed + 11)
+    db = dbformat.build_from_arrays(res, lens)
+    db.SA = gpu_sa.suffix_array(db.T, dev)
+    torch.cuda.empty_cache()
+    qres, qlens = synth.search_queries_arrays(res, lens, 5000, 5000, seed=args.seed + 12)
+    qoff = np.cumsum(qlens) - qlens
+    q_aa = [qres[o:o + n].tobytes() for o, n in zip(qoff, qlens)]
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ix = native.Index(db)
+    load_s = time.perf_counter() - t0
+    mat = synth.matrix("BLOSUM62")
+    ix.search([native.prepare_query(q) for q in q_aa[:200]], mat)          # warm-up
+    torch.cuda.synchronize()
+    bsz = args.search_batch
+    stage = np.zeros(4)
+    nh = nsw = 0
+    t0 = time.perf_counter()
+    for b in range(0, len(q_aa), bsz):
+        qs = [native.prepare_query(q) for q in q_aa[b:b + bsz]]
+        r = ix.search(qs, mat)
+        stage += np.array(r["stage_ms"])
+        nh += len(r["protein"])
+        nsw += int((r["sw_status"] == native.TPZ_SW_OK).sum())
+    wall = time.perf_counter() - t0
+    out = {"workload": SEARCH_WORKLOAD % bsz, "queries": len(q_aa), "queries_per_s": round(len(q_aa) / wall, 1),
+           "wall_s": round(wall, 3),
+           "api": "tpz_search_batch (host buffers; SEG + alphabet on the host inside the timed region)",
+           "device_ms": {"seed": round(stage[0], 2), "walk_hitlist": round(stage[1], 2),
+                         "sw_of_hits": round(stage[2], 2), "calls_wall": round(stage[3], 2)},
+           "hits_per_query": round(nh / len(q_aa), 1), "sw_pairs_per_query": round(nsw / len(q_aa), 1),
+           "setup_s": round(setup_s, 1), "index_load_s": round(load_s, 2),
+           "index_device_gb": round(ix.device_bytes / 1e9, 2)}
+    ix.close()
+    if args.no_cpu_baseline or not os.path.exists(oracle.REF_BIN):
+        return out
+    # the reference binary on a query sample, all host threads; our CLI on the
+    # same sample; outputs compared per query block
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as tmp:
+        pre = os.path.join(tmp, "db")
+        dbformat.write_files(pre, db)
+
+        def run(exe, n):
+            fa = os.path.join(tmp, "q%d.fa" % n)
+            synth.write_fasta(fa, synth.Proteins(["q%d" % i for i in range(n)],
+                                                 [np.frombuffer(q, np.uint8) for q in q_aa[:n]]))
+            t = time.perf_counter()
+            r = subprocess.run([exe, "search", "-f", fa, "-p", pre, "-T", str(threads)],
+                               capture_output=True, cwd=tmp)
+            return time.perf_counter() - t, r
+
+        dt, _ = run(oracle.REF_BIN, 4 * threads)
+        n = int(min(len(q_aa), max(4 * threads, 4 * threads * 15.0 / max(dt, 1e-3))))
+        dt, rr = run(oracle.REF_BIN, n)
+        _, rm = run(B.CLI, n)
+
+        def blocks(text):
+            d = {}
+            for ln in text.decode().splitlines()[1:]:
+                d.setdefault(ln.split("\t", 1)[0], []).append(ln)
+            return d
+        out["cpu_reference"] = {"queries_per_s": round(n / dt, 2), "threads": threads,
+                                "kind": "reference", "sample": "first %d queries, topaz search -T %d, "
+                                "DB files in page cache" % (n, threads)}
+        out["parity_sample"] = {"queries": n, "identical_blocks": blocks(rr.stdout) == blocks(rm.stdout),
+                                "lines": rr.stdout.count(b"\n") - 1}
+    return out
 
 
 def native_arm(args, rank, local_rank, world):
@@ -244,6 +339,11 @@ def native_arm(args, rank, local_rank, world):
     d2h = sum(v.numel() * v.element_size() for v in outs.values())
 
     line = None
+    search = None
+    if rank == 0 and world == 1 and not args.no_search:
+        del t, pin, outs
+        torch.cuda.empty_cache()
+        search = search_bench(args, dev)
     if rank == 0:
         cpu = None if args.no_cpu_baseline else cpu_baseline_sw(ps, mat)
         traffic_per_cell = read_traffic()
@@ -268,6 +368,7 @@ def native_arm(args, rank, local_rank, world):
             "cpu_baseline": cpu,
             "clocks": clk,
             "step_ms": [round(x, 3) for x in step_ms],
+            "search": search,
         }
     if world > 1:
         dist.barrier()

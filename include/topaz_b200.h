@@ -182,6 +182,8 @@ typedef struct {
     const int64_t *trace_n;                  /* nq (when trace_pops > 0) */
     const int64_t *trace_row;                /* nq * trace_pops */
     const int32_t *trace_off, *trace_score, *trace_len, *trace_counted;
+    double stage_ms[4];      /* device time: seed lookup, walk + hitlist, SW of hits;
+                                [3] = host wall time of the whole call incl. copies */
 } tpz_search_result;
 
 TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,

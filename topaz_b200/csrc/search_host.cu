@@ -3,6 +3,7 @@
 #include <stddef.h>
 #include <stdio.h>
 #include <string.h>
+#include <sys/time.h>
 
 #include <algorithm>
 #include <string>
@@ -355,8 +356,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     while (hash_size < 2 * (max_cap + 1)) hash_size <<= 1;
     auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
     const size_t ns = (size_t)max_cap + 1;
-    const size_t per_q = al(4 * (size_t)max_cursors) + al(4 * (size_t)kSMax) + al(8 * (kSMax / 64)) +
-                         7 * al(4 * ns) + 2 * al(4 * (size_t)kSMax) + al(8 * (kSMax / 64)) +
+    const size_t per_q = 7 * al(4 * ns) + 2 * al(4 * (size_t)kSMax) + al(8 * (kSMax / 64)) +
                          2 * al(4 * (size_t)hash_size);
 
     int8_t sub[625], xmap[128];
@@ -366,12 +366,14 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     DevBuf b;
     uint8_t *dq, *dscratch; int64_t *dqo, *dpb, *dcb; int32_t *dql, *dqs; int8_t *dsub;
     Cursor *dcur; Hit *dhits; QueryOut *dqout; PopRec *dtrace = nullptr;
+    int32_t *dqnext; uint32_t *dcache;
     int rc;
     if ((rc = b.alloc(&dq, bytes + 1)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
         (rc = b.alloc(&dpb, nq + 1)) || (rc = b.alloc(&dcb, nq + 1)) || (rc = b.alloc(&dqs, nq)) ||
         (rc = b.alloc(&dsub, 625)) || (rc = b.alloc(&dcur, 2 * npos + 1)) ||
         (rc = b.alloc(&dscratch, per_q * nq)) || (rc = b.alloc(&dhits, (size_t)nq * max_cap)) ||
-        (rc = b.alloc(&dqout, nq)))
+        (rc = b.alloc(&dqout, nq)) || (rc = b.alloc(&dqnext, 2 * npos + 1)) ||
+        (rc = b.alloc(&dcache, 32 * (2 * npos + 1))))
         return rc;
     if (o->trace_pops > 0 && (rc = b.alloc(&dtrace, (size_t)nq * o->trace_pops))) return rc;
     TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
@@ -383,6 +385,12 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     TPZ_CUDA(cudaMemcpy(dsub, sub, 625, cudaMemcpyHostToDevice));
 
     const int nsm = tpz::sm_count();
+    struct timeval tw0, tw1;
+    gettimeofday(&tw0, nullptr);
+    cudaEvent_t ev[4];
+    for (auto &e : ev) TPZ_CUDA(cudaEventCreate(&e));
+    struct EvFree { cudaEvent_t *e; ~EvFree() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); } } evfree{ev};
+    TPZ_CUDA(cudaEventRecord(ev[0], 0));
     if (npos > 0) {
         SeedArgs sa;
         sa.qcat = dq; sa.qoff = dqo; sa.qlen = dql; sa.pos_base = dpb; sa.nq = (int)nq;
@@ -396,8 +404,11 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     wa.max_cap = max_cap; wa.hash_size = hash_size; wa.max_cursors = max_cursors;
     wa.scratch = dscratch; wa.scratch_per_query = per_q; wa.hits = dhits; wa.qout = dqout;
     wa.qstatus = dqs; wa.trace = dtrace; wa.trace_cap = o->trace_pops;
-    walk_kernel<<<(unsigned)((nq + 31) / 32), 32>>>(ix->d, wa);
+    wa.qnext = dqnext; wa.ccache = dcache;
+    TPZ_CUDA(cudaEventRecord(ev[1], 0));
+    walk_kernel<<<(unsigned)((nq + kWalkWarps - 1) / kWalkWarps), kWalkWarps * 32>>>(ix->d, wa);
     TPZ_CUDA(cudaGetLastError());
+    TPZ_CUDA(cudaEventRecord(ev[2], 0));
 
     ResultHolder *R = new ResultHolder();
     std::vector<QueryOut> qo(nq);
@@ -449,6 +460,8 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
             scatter_sw_kernel<<<(unsigned)std::min<int64_t>((npairs + 255) / 256, 4096), 256>>>(
                 npairs, p_hit, sc, re, rd, st, raw, send, qend, psw);
         }
+        if (cudaEventRecord(ev[3], 0) != cudaSuccess)
+            return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch event"));
         if (cudaMemcpy(R->protein.data(), pprot, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
             cudaMemcpy(R->gs.data(), pgs, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
             cudaMemcpy(R->gl.data(), pgl, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
@@ -485,6 +498,15 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     r.trace_len = o->trace_pops > 0 ? R->trace_len.data() : nullptr;
     r.trace_counted = o->trace_pops > 0 ? R->trace_counted.data() : nullptr;
     TPZ_CUDA(cudaDeviceSynchronize());
+    float t01 = 0, t12 = 0, t23 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    if (nh > 0) cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    gettimeofday(&tw1, nullptr);
+    r.stage_ms[0] = t01;
+    r.stage_ms[1] = t12;
+    r.stage_ms[2] = t23;
+    r.stage_ms[3] = (tw1.tv_sec - tw0.tv_sec) * 1e3 + (tw1.tv_usec - tw0.tv_usec) / 1e3;
     *out = &R->r;
     return TPZ_OK;
 }

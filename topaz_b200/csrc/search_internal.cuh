@@ -21,8 +21,13 @@ struct DevIndex {
 
 struct Cursor {
     int64_t row;
-    int32_t off, dir, score, len;
+    int32_t off;
+    int16_t dir;
+    uint8_t cpos, cn;    // next unused / valid entries of the cursor's element cache
+    int32_t score, len;
 };
+
+constexpr int kWalkWarps = 4;            // queries (warps) per walk block
 
 struct Hit {
     int32_t protein, gapless_score, gapless_length, suffix_offset;
@@ -61,8 +66,10 @@ struct WalkArgs {
     const int8_t *sub;
     int min_hit_length, seeds, alignments, num_hits;
     int max_cap, hash_size, max_cursors;
-    uint8_t *scratch;
+    uint8_t *scratch;             // per query: hitlist structures
     size_t scratch_per_query;
+    int32_t *qnext;               // per cursor (global cursor index)
+    uint32_t *ccache;             // 32 packed chain elements per cursor
     Hit *hits;                    // nq * max_cap
     QueryOut *qout;
     const int32_t *qstatus;

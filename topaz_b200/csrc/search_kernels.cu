@@ -200,8 +200,8 @@ __global__ void seed_kernel(DevIndex ix, SeedArgs a) {
         const uint8_t *Q = a.qcat + a.qoff[q];
         const int qlen = a.qlen[q];
         Cursor c0, c1;
-        c0.row = -1; c0.off = i; c0.dir = 1; c0.score = 0; c0.len = -1;
-        c1.row = -1; c1.off = i; c1.dir = -1; c1.score = 0; c1.len = -1;
+        c0.row = -1; c0.off = i; c0.dir = 1; c0.cpos = 0; c0.cn = 0; c0.score = 0; c0.len = -1;
+        c1.row = -1; c1.off = i; c1.dir = -1; c1.cpos = 0; c1.cn = 0; c1.score = 0; c1.len = -1;
         if (Q[i] != 'V') {                     // _bad_prefix: internal 'V' = X
             const int64_t pos = lower_bound(ix, Q + i, qlen - i);
             if (a.lb_out) a.lb_out[g] = pos;
@@ -251,43 +251,6 @@ __global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t
 
 // ------------------------------------------------------------------ walk
 
-struct WalkView {
-    // cursor queue
-    int32_t *qnext;        // ncur: next cursor in the same score stack
-    int32_t *qhead;        // kSMax: top of each score stack (-1 empty)
-    uint64_t *qbits;       // kSMax/64: non-empty stacks
-    // hitlist
-    int32_t *hprot, *hscore, *hlen, *hoff, *hprev, *hnext;   // cap+1 slots
-    int32_t *hfree;        // free slot stack
-    int32_t *bhead, *btail;   // kSMax per-score lists (head = oldest)
-    uint64_t *bbits;
-    int32_t *hkey, *hval;  // hash (hsize entries)
-};
-
-__device__ __forceinline__ WalkView walk_view(const WalkArgs &a, int q) {
-    uint8_t *base = a.scratch + (size_t)q * a.scratch_per_query;
-    WalkView v;
-    size_t o = 0;
-    auto take = [&](size_t bytes) { uint8_t *p = base + o; o += (bytes + 15) & ~(size_t)15; return p; };
-    v.qnext = (int32_t *)take(4 * (size_t)a.max_cursors);
-    v.qhead = (int32_t *)take(4 * (size_t)kSMax);
-    v.qbits = (uint64_t *)take(8 * (size_t)(kSMax / 64));
-    const size_t ns = (size_t)a.max_cap + 1;
-    v.hprot = (int32_t *)take(4 * ns);
-    v.hscore = (int32_t *)take(4 * ns);
-    v.hlen = (int32_t *)take(4 * ns);
-    v.hoff = (int32_t *)take(4 * ns);
-    v.hprev = (int32_t *)take(4 * ns);
-    v.hnext = (int32_t *)take(4 * ns);
-    v.hfree = (int32_t *)take(4 * ns);
-    v.bhead = (int32_t *)take(4 * (size_t)kSMax);
-    v.btail = (int32_t *)take(4 * (size_t)kSMax);
-    v.bbits = (uint64_t *)take(8 * (size_t)(kSMax / 64));
-    v.hkey = (int32_t *)take(4 * (size_t)a.hash_size);
-    v.hval = (int32_t *)take(4 * (size_t)a.hash_size);
-    return v;
-}
-
 __device__ __forceinline__ uint32_t hash32(uint32_t x) {
     x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
     return x;
@@ -316,184 +279,282 @@ __device__ __forceinline__ int bits_min_ge(const uint64_t *bits, int from, int n
     }
 }
 
-// One thread per query: the pop loop of query_fetch_alignment_batch
-// (src/query.c:151-157) over pqueue_next (priority_queue.c:36-56) and
-// hitlist_add (hit.c:126-193).
-__global__ void walk_kernel(DevIndex ix, WalkArgs a) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+// packed chain element: score in the low half, length in the high half
+constexpr int kLenEnd = -1000;      // row outside [0, 8*Tsize): the cursor is freed
+constexpr int kLenFault = -2000;    // row past the zero-filled SA page
+__device__ __forceinline__ uint32_t pack_elem(int score, int len) {
+    return (uint32_t)(uint16_t)(int16_t)score | ((uint32_t)(uint16_t)(int16_t)len << 16);
+}
+__device__ __forceinline__ int elem_score(uint32_t e) { return (int)(int16_t)(e & 0xFFFFu); }
+__device__ __forceinline__ int elem_len(uint32_t e) { return (int)(int16_t)(e >> 16); }
+
+struct HitView {
+    int32_t *hprot, *hscore, *hlen, *hoff, *hprev, *hnext, *hfree;   // cap+1 slots
+    int32_t *bhead, *btail;      // kSMax per-score lists (head = oldest)
+    uint64_t *bbits;
+    int32_t *hkey, *hval;        // protein -> slot, open addressing
+};
+
+__device__ __forceinline__ HitView hit_view(const WalkArgs &a, int q) {
+    uint8_t *base = a.scratch + (size_t)q * a.scratch_per_query;
+    HitView v;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { uint8_t *p = base + o; o += (bytes + 15) & ~(size_t)15; return p; };
+    const size_t ns = (size_t)a.max_cap + 1;
+    v.hprot = (int32_t *)take(4 * ns);
+    v.hscore = (int32_t *)take(4 * ns);
+    v.hlen = (int32_t *)take(4 * ns);
+    v.hoff = (int32_t *)take(4 * ns);
+    v.hprev = (int32_t *)take(4 * ns);
+    v.hnext = (int32_t *)take(4 * ns);
+    v.hfree = (int32_t *)take(4 * ns);
+    v.bhead = (int32_t *)take(4 * (size_t)kSMax);
+    v.btail = (int32_t *)take(4 * (size_t)kSMax);
+    v.bbits = (uint64_t *)take(8 * (size_t)(kSMax / 64));
+    v.hkey = (int32_t *)take(4 * (size_t)a.hash_size);
+    v.hval = (int32_t *)take(4 * (size_t)a.hash_size);
+    return v;
+}
+
+// One warp per query.  Lane 0 runs the pop loop of
+// query_fetch_alignment_batch (src/query.c:151-157) over pqueue_next
+// (priority_queue.c:36-56) and hitlist_add (hit.c:126-193) exactly, with the
+// per-score cursor stacks in shared memory.  A cursor's next chain elements
+// (sa_hsp at rows row+dir, row+2dir, ...) come from a 32-entry per-cursor
+// cache that all 32 lanes refill in one go whenever lane 0 pops a cursor
+// whose cache is used up, so consecutive pops of a cursor cost no sa_hsp.
+// Elements past the end of a chain are computed and never used.
+__global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, WalkArgs a) {
+    constexpr int NW = kSMax / 64;
+    __shared__ int16_t s_qhead[kWalkWarps][kSMax];
+    __shared__ uint64_t s_qbits[kWalkWarps][NW];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int q = blockIdx.x * kWalkWarps + wib;
     if (q >= a.nq) return;
-    WalkView v = walk_view(a, q);
+    int16_t *qhead = s_qhead[wib];
+    uint64_t *qbits = s_qbits[wib];
     const uint8_t *Q = a.qcat + a.qoff[q];
     const int qlen = a.qlen[q];
     const int minlen = a.min_hit_length;
     const int64_t cbase = a.cursor_base[q];
     const int ncur = (int)(a.cursor_base[q + 1] - cbase);
     Cursor *cur = a.cursors + cbase;
-    constexpr int NW = kSMax / 64;
+    int32_t *qnext = a.qnext + cbase;
+    uint32_t *cache = a.ccache + cbase * 32;
+    HitView v = hit_view(a, q);
+    const int cap = qlen > 3000 ? (int)(1.5 * a.num_hits) : a.alignments;   // hit.c:106-109
 
-    // ---- queue init, in seeding insertion order
-    for (int i = 0; i < kSMax; ++i) v.qhead[i] = -1;
-    for (int i = 0; i < NW; ++i) v.qbits[i] = 0;
+    // ---- cooperative initialisation
+    for (int i = lane; i < kSMax; i += 32) {
+        qhead[i] = -1;
+        v.bhead[i] = -1;
+        v.btail[i] = -1;
+    }
+    for (int i = lane; i < NW; i += 32) { qbits[i] = 0; v.bbits[i] = 0; }
+    for (int i = lane; i < a.hash_size; i += 32) v.hkey[i] = -1;
+    for (int i = lane; i <= cap; i += 32) v.hfree[i] = cap - i;
+    __syncwarp();
+
     int qmax = -1;
     int64_t qsize = 0;
-    for (int c = 0; c < ncur; ++c) {
-        if (cur[c].len >= minlen) {
-            const int s = cur[c].score;
-            v.qnext[c] = v.qhead[s];
-            v.qhead[s] = c;
-            v.qbits[s >> 6] |= 1ull << (s & 63);
-            if (s > qmax) qmax = s;
-            ++qsize;
-        }
-    }
-
-    // ---- hitlist init
-    const int cap = qlen > 3000 ? (int)(1.5 * a.num_hits) : a.alignments;   // hit.c:106-109
-    for (int i = 0; i < kSMax; ++i) { v.bhead[i] = -1; v.btail[i] = -1; }
-    for (int i = 0; i < NW; ++i) v.bbits[i] = 0;
-    for (int i = 0; i < a.hash_size; ++i) v.hkey[i] = -1;
-    for (int i = 0; i <= cap; ++i) v.hfree[i] = cap - i;
-    int nfree = cap + 1;
-    int hsize = 0;
-    int hmin = kSMax;     // smallest non-empty score list (kSMax = none)
+    int nfree = cap + 1, hsize = 0, hmin = kSMax;
     const uint32_t hmask = (uint32_t)a.hash_size - 1;
-
     int64_t npops = 0, counter = 0;
     int status = 0;
     PopRec *trace = a.trace ? a.trace + (int64_t)q * a.trace_cap : nullptr;
-
-    while (qsize > 0) {
-        // ---- pqueue_next: pop the newest cursor of the highest score
-        const int s = qmax;
-        const int c = v.qhead[s];
-        v.qhead[s] = v.qnext[c];
-        if (v.qhead[s] < 0) {
-            v.qbits[s >> 6] &= ~(1ull << (s & 63));
-            qmax = s > 0 ? bits_max_le(v.qbits, s - 1) : -1;
-        }
-        --qsize;
-        const int64_t row = cur[c].row;
-        const int gs = cur[c].score, gl = cur[c].len, off = cur[c].off;
-        // suffix_increment + suffix_active: advance and re-insert
-        const int64_t nr = row + cur[c].dir;
-        if (nr >= 0 && nr < 8 * ix.Tsize) {
-            if (nr >= ix.sa_rows) {
-                status |= TPZ_Q_SA_END;
-                break;
-            }
-            int sc = cur[c].score;
-            const int ln = hsp_at(ix, ix.SA[nr], Q, qlen, off, a.sub, &sc);
-            cur[c].row = nr;
-            cur[c].len = ln;
-            if (ln >= minlen) {
-                cur[c].score = sc;
-                v.qnext[c] = v.qhead[sc];
-                v.qhead[sc] = c;
-                v.qbits[sc >> 6] |= 1ull << (sc & 63);
+    if (lane == 0) {
+        // the queue in seeding insertion order
+        for (int c = 0; c < ncur; ++c) {
+            if (cur[c].len >= minlen) {
+                const int sc = cur[c].score;
+                qnext[c] = qhead[sc];
+                qhead[sc] = (int16_t)c;
+                qbits[sc >> 6] |= 1ull << (sc & 63);
                 if (sc > qmax) qmax = sc;
                 ++qsize;
             }
         }
+    }
 
-        // ---- hitlist_add
-        bool counted = false;
-        if (hsize >= cap && hmin >= gs) {
-            counted = true;            // full and the worst hit is at least as good
-        } else {
-            if (row >= ix.sa_rows) { status |= TPZ_Q_SA_END; break; }
-            const int p = (int)protein_of(ix, ix.SA[row]);
-            uint32_t hh = hash32((uint32_t)p) & hmask;
-            while (v.hkey[hh] != -1 && v.hkey[hh] != p) hh = (hh + 1) & hmask;
-            if (v.hkey[hh] == -1) {
-                // new protein: newest entry of its score list
-                const int slot = v.hfree[--nfree];
-                v.hprot[slot] = p; v.hscore[slot] = gs; v.hlen[slot] = gl; v.hoff[slot] = off;
-                v.hnext[slot] = -1;
-                v.hprev[slot] = v.btail[gs];
-                if (v.btail[gs] >= 0) v.hnext[v.btail[gs]] = slot; else v.bhead[gs] = slot;
-                v.btail[gs] = slot;
-                v.bbits[gs >> 6] |= 1ull << (gs & 63);
-                if (gs < hmin) hmin = gs;
-                v.hkey[hh] = p; v.hval[hh] = slot;
-                ++hsize;
-                if (hsize > cap) {
-                    // evict the oldest entry of the smallest score
-                    const int m = hmin;
-                    const int w = v.bhead[m];
-                    v.bhead[m] = v.hnext[w];
-                    if (v.bhead[m] >= 0) v.hprev[v.bhead[m]] = -1; else {
-                        v.btail[m] = -1;
-                        v.bbits[m >> 6] &= ~(1ull << (m & 63));
-                        const int nm = bits_min_ge(v.bbits, m + 1, NW);
-                        hmin = nm < 0 ? kSMax : nm;
-                    }
-                    // delete its protein from the table (backward shift)
-                    const int wp = v.hprot[w];
-                    uint32_t i = hash32((uint32_t)wp) & hmask;
-                    while (v.hkey[i] != wp) i = (i + 1) & hmask;
-                    uint32_t j = i;
-                    for (;;) {
-                        j = (j + 1) & hmask;
-                        if (v.hkey[j] == -1) break;
-                        const uint32_t k = hash32((uint32_t)v.hkey[j]) & hmask;
-                        // move j into the hole at i when its home k is not in (i, j]
-                        const bool stay = (i <= j) ? (i < k && k <= j) : (i < k || k <= j);
-                        if (!stay) {
-                            v.hkey[i] = v.hkey[j]; v.hval[i] = v.hval[j];
-                            i = j;
-                        }
-                    }
-                    v.hkey[i] = -1;
-                    v.hfree[nfree++] = w;
-                    --hsize;
-                }
-                counted = true;
+    for (;;) {
+        // ---- lane 0: pop the newest cursor of the highest score
+        int c = -1, need = 0, off = 0, dir = 0;
+        int64_t row = 0;
+        Cursor cc;
+        if (lane == 0 && qsize > 0) {
+            const int s = qmax;
+            c = qhead[s];
+            cc = cur[c];
+            const int nx = qnext[c];
+            qhead[s] = (int16_t)nx;
+            if (nx < 0) {
+                qbits[s >> 6] &= ~(1ull << (s & 63));
+                qmax = s > 0 ? bits_max_le(qbits, s - 1) : -1;
+            }
+            --qsize;
+            row = cc.row; off = cc.off; dir = cc.dir;
+            need = cc.cpos >= cc.cn;
+        }
+        c = __shfl_sync(0xFFFFFFFFu, c, 0);
+        if (c < 0) break;
+        need = __shfl_sync(0xFFFFFFFFu, need, 0);
+        uint32_t elem = 0;
+        if (need) {
+            // all lanes: the next 32 rows of this cursor
+            row = __shfl_sync(0xFFFFFFFFu, row, 0);
+            off = __shfl_sync(0xFFFFFFFFu, off, 0);
+            dir = __shfl_sync(0xFFFFFFFFu, dir, 0);
+            const int64_t nr = row + (int64_t)dir * (lane + 1);
+            if (nr < 0 || nr >= 8 * ix.Tsize) {
+                elem = pack_elem(0, kLenEnd);
+            } else if (nr >= ix.sa_rows) {
+                elem = pack_elem(0, kLenFault);
             } else {
-                const int h = v.hval[hh];
-                const int os = v.hscore[h];
-                if (os < gs) {
-                    // rb_reput: unlink, re-key, append as newest
-                    if (v.hprev[h] >= 0) v.hnext[v.hprev[h]] = v.hnext[h]; else v.bhead[os] = v.hnext[h];
-                    if (v.hnext[h] >= 0) v.hprev[v.hnext[h]] = v.hprev[h]; else v.btail[os] = v.hprev[h];
-                    if (v.bhead[os] < 0) {
-                        v.bbits[os >> 6] &= ~(1ull << (os & 63));
-                        if (hmin == os) {
-                            const int nm = bits_min_ge(v.bbits, os + 1, NW);
-                            hmin = nm < 0 ? kSMax : nm;
+                int sc = 0;
+                const int ln = hsp_at(ix, ix.SA[nr], Q, qlen, off, a.sub, &sc);
+                elem = pack_elem(sc, ln);
+            }
+            cache[(int64_t)c * 32 + lane] = elem;
+            __syncwarp();
+        }
+        int stop = 0;
+        if (lane == 0) {
+            if (need) {
+                cc.cpos = 1;
+                cc.cn = 32;
+            } else {
+                elem = cache[(int64_t)c * 32 + cc.cpos];
+                cc.cpos++;
+            }
+            const int gs = cc.score, gl = cc.len;
+            // suffix_increment + suffix_active
+            const int ln = elem_len(elem);
+            if (ln == kLenFault) {
+                status |= TPZ_Q_SA_END;
+                stop = 1;
+            } else {
+                if (ln != kLenEnd) {
+                    cc.row = row + dir;
+                    cc.len = ln;
+                    if (ln >= minlen) {
+                        const int sc = elem_score(elem);
+                        cc.score = sc;
+                        qnext[c] = qhead[sc];
+                        qhead[sc] = (int16_t)c;
+                        qbits[sc >> 6] |= 1ull << (sc & 63);
+                        if (sc > qmax) qmax = sc;
+                        ++qsize;
+                    }
+                }
+                cur[c] = cc;
+
+                // ---- hitlist_add (every queued row is below sa_rows: seeding and
+                // the advance above stop at the first row past it)
+                bool counted = false;
+                if (hsize >= cap && hmin >= gs) {
+                    counted = true;            // full and the worst hit is at least as good
+                } else {
+                    const int p = (int)protein_of(ix, ix.SA[row]);
+                    uint32_t hh = hash32((uint32_t)p) & hmask;
+                    while (v.hkey[hh] != -1 && v.hkey[hh] != p) hh = (hh + 1) & hmask;
+                    if (v.hkey[hh] == -1) {
+                        // new protein: newest entry of its score list
+                        const int slot = v.hfree[--nfree];
+                        v.hprot[slot] = p; v.hscore[slot] = gs; v.hlen[slot] = gl; v.hoff[slot] = off;
+                        v.hnext[slot] = -1;
+                        v.hprev[slot] = v.btail[gs];
+                        if (v.btail[gs] >= 0) v.hnext[v.btail[gs]] = slot; else v.bhead[gs] = slot;
+                        v.btail[gs] = slot;
+                        v.bbits[gs >> 6] |= 1ull << (gs & 63);
+                        if (gs < hmin) hmin = gs;
+                        v.hkey[hh] = p; v.hval[hh] = slot;
+                        ++hsize;
+                        if (hsize > cap) {
+                            // evict the oldest entry of the smallest score
+                            const int m = hmin;
+                            const int w = v.bhead[m];
+                            v.bhead[m] = v.hnext[w];
+                            if (v.bhead[m] >= 0) v.hprev[v.bhead[m]] = -1; else {
+                                v.btail[m] = -1;
+                                v.bbits[m >> 6] &= ~(1ull << (m & 63));
+                                const int nm = bits_min_ge(v.bbits, m + 1, NW);
+                                hmin = nm < 0 ? kSMax : nm;
+                            }
+                            // delete its protein from the table (backward shift)
+                            const int wp = v.hprot[w];
+                            uint32_t i = hash32((uint32_t)wp) & hmask;
+                            while (v.hkey[i] != wp) i = (i + 1) & hmask;
+                            uint32_t j = i;
+                            for (;;) {
+                                j = (j + 1) & hmask;
+                                if (v.hkey[j] == -1) break;
+                                const uint32_t k = hash32((uint32_t)v.hkey[j]) & hmask;
+                                // move j into the hole at i when its home k is not in (i, j]
+                                const bool keep = (i <= j) ? (i < k && k <= j) : (i < k || k <= j);
+                                if (!keep) {
+                                    v.hkey[i] = v.hkey[j]; v.hval[i] = v.hval[j];
+                                    i = j;
+                                }
+                            }
+                            v.hkey[i] = -1;
+                            v.hfree[nfree++] = w;
+                            --hsize;
+                        }
+                        counted = true;
+                    } else {
+                        const int h = v.hval[hh];
+                        const int os = v.hscore[h];
+                        if (os < gs) {
+                            // rb_reput: unlink, re-key, append as newest
+                            if (v.hprev[h] >= 0) v.hnext[v.hprev[h]] = v.hnext[h]; else v.bhead[os] = v.hnext[h];
+                            if (v.hnext[h] >= 0) v.hprev[v.hnext[h]] = v.hprev[h]; else v.btail[os] = v.hprev[h];
+                            if (v.bhead[os] < 0) {
+                                v.bbits[os >> 6] &= ~(1ull << (os & 63));
+                                if (hmin == os) {
+                                    const int nm = bits_min_ge(v.bbits, os + 1, NW);
+                                    hmin = nm < 0 ? kSMax : nm;
+                                }
+                            }
+                            v.hscore[h] = gs; v.hlen[h] = gl;
+                            v.hnext[h] = -1;
+                            v.hprev[h] = v.btail[gs];
+                            if (v.btail[gs] >= 0) v.hnext[v.btail[gs]] = h; else v.bhead[gs] = h;
+                            v.btail[gs] = h;
+                            v.bbits[gs >> 6] |= 1ull << (gs & 63);
+                            if (gs < hmin) hmin = gs;
                         }
                     }
-                    v.hscore[h] = gs; v.hlen[h] = gl;
-                    v.hnext[h] = -1;
-                    v.hprev[h] = v.btail[gs];
-                    if (v.btail[gs] >= 0) v.hnext[v.btail[gs]] = h; else v.bhead[gs] = h;
-                    v.btail[gs] = h;
-                    v.bbits[gs >> 6] |= 1ull << (gs & 63);
-                    if (gs < hmin) hmin = gs;
                 }
+                if (trace && npops < a.trace_cap) {
+                    PopRec r; r.row = row; r.off = off; r.score = gs; r.len = gl; r.counted = counted;
+                    trace[npops] = r;
+                }
+                ++npops;
+                if (counted && ++counter == a.seeds) stop = 1;
             }
         }
-        if (trace && npops < a.trace_cap) {
-            PopRec r; r.row = row; r.off = off; r.score = gs; r.len = gl; r.counted = counted;
-            trace[npops] = r;
-        }
-        ++npops;
-        if (counted && ++counter == a.seeds) break;
+        stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
+        if (stop) break;
     }
 
-    // ---- hitlist in traversal order: score descending, newest first
-    Hit *out = a.hits + (int64_t)q * a.max_cap;
-    int n = 0;
-    for (int sc = bits_max_le(v.bbits, kSMax - 1); sc >= 0; sc = sc > 0 ? bits_max_le(v.bbits, sc - 1) : -1) {
-        for (int h = v.btail[sc]; h >= 0; h = v.hprev[h]) {
-            Hit o;
-            o.protein = v.hprot[h]; o.gapless_score = v.hscore[h]; o.gapless_length = v.hlen[h];
-            o.suffix_offset = v.hoff[h];
-            out[n++] = o;
+    if (lane == 0) {
+        // ---- hitlist in traversal order: score descending, newest first
+        Hit *out = a.hits + (int64_t)q * a.max_cap;
+        int n = 0;
+        for (int sc = bits_max_le(v.bbits, kSMax - 1); sc >= 0;
+             sc = sc > 0 ? bits_max_le(v.bbits, sc - 1) : -1) {
+            for (int h = v.btail[sc]; h >= 0; h = v.hprev[h]) {
+                Hit o;
+                o.protein = v.hprot[h]; o.gapless_score = v.hscore[h]; o.gapless_length = v.hlen[h];
+                o.suffix_offset = v.hoff[h];
+                out[n++] = o;
+            }
         }
+        QueryOut qo;
+        qo.nhits = n; qo.npops = npops; qo.ncounted = counter; qo.status = status | a.qstatus[q];
+        a.qout[q] = qo;
     }
-    QueryOut qo;
-    qo.nhits = n; qo.npops = npops; qo.ncounted = counter; qo.status = status | a.qstatus[q];
-    a.qout[q] = qo;
 }
 
 }  // namespace search

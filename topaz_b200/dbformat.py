@@ -51,11 +51,10 @@ class Database:
 def parse_fasta(data: bytes):
     """fasta_next/_create_seq (src/fasta.c:80-120, :62-78) record splitting.
 
-    A record runs from a '>' that starts the file or follows '\\n' to the
-    byte before the next such '>'; the last record drops the file's final
-    byte.  The ID is the header up to the first space/tab (src/seq.c:55-78);
-    the residues are every non-'\\n' byte after the header line, upper-cased
-    by upper_aa (src/seq.c:80-104)."""
+    A record runs from a '>' that starts the file or follows '\\n' up to the
+    next such '>'.  The ID is the header up to the first space/tab
+    (src/seq.c:55-78); the residues are every non-'\\n' byte after the
+    header line, upper-cased by upper_aa (src/seq.c:80-104)."""
     out = []
     n = len(data)
     if n == 0:
@@ -126,3 +125,24 @@ def read_files(prefix: str) -> Database:
 
 def exists(prefix: str) -> bool:
     return all(os.path.exists(prefix + e) for e in (".psq", ".SA", ".phr", ".ind"))
+
+
+def build_from_arrays(residues: np.ndarray, lens: np.ndarray, id_prefix: str = "db") -> Database:
+    """T, .ind and .phr for proteins given as concatenated upper-case residues
+    and lengths (ids id_prefix0, id_prefix1, ...), without per-protein loops."""
+    lens = np.asarray(lens, dtype=np.int64)
+    n = len(lens)
+    internal = ab.aa_to_internal(residues)
+    pstart = np.cumsum(lens + 1) - (lens + 1)
+    T = np.full(int(lens.sum()) + n, ord("\n"), dtype=np.uint8)
+    pos = np.repeat(pstart - (np.cumsum(lens) - lens), lens) + np.arange(int(lens.sum()))
+    T[pos] = internal
+    ids = [("%s%d" % (id_prefix, i)).encode() for i in range(n)]
+    hl = np.array([len(x) for x in ids], dtype=np.int64)
+    hs = np.cumsum(hl + 1) - (hl + 1)
+    ind = np.zeros(n, dtype=IND_DTYPE)
+    ind["header_start"] = hs
+    ind["protein_start"] = pstart
+    ind["header_len"] = hl
+    ind["protein_len"] = lens
+    return Database(T, None, ind, b"\n".join(ids) + b"\n")

@@ -139,7 +139,7 @@ class _SearchResult(ctypes.Structure):
                 ("suffix_offset", _P32), ("rawscore", _P32), ("qend", _P32), ("send", _P32),
                 ("sw_status", _P32), ("trace_n", _P64), ("trace_row", _P64),
                 ("trace_off", _P32), ("trace_score", _P32), ("trace_len", _P32),
-                ("trace_counted", _P32)]
+                ("trace_counted", _P32), ("stage_ms", ctypes.c_double * 4)]
 
 
 def _search_sigs(L):
@@ -247,6 +247,7 @@ class Index:
             for k in ("protein", "gapless_score", "gapless_length", "suffix_offset", "rawscore",
                       "qend", "send", "sw_status"):
                 out[k] = arr(getattr(r, k), nh)
+            out["stage_ms"] = list(r.stage_ms)
             if trace_pops:
                 out["trace_n"] = arr(r.trace_n, nq)
                 for k in ("trace_row", "trace_off", "trace_score", "trace_len", "trace_counted"):
@@ -264,3 +265,21 @@ def karlin(qlen, db_size, db_proteins, raw, lam=0.267, k=0.041, H=0.14):
     L.tpz_karlin(int(qlen), int(db_size), int(db_proteins), lam, k, H, int(raw),
                  ctypes.byref(b), ctypes.byref(e))
     return b.value, e.value
+
+
+def seg_mask(residues: bytes) -> bytes:
+    """SEG hard-masking of upper-cased residues (tpzh_seg_mask)."""
+    L = lib()
+    L.tpzh_seg_mask.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    buf = ctypes.create_string_buffer(residues, len(residues))
+    L.tpzh_seg_mask(buf, len(residues))
+    return buf.raw[:len(residues)]
+
+
+def prepare_query(residues: bytes, seg: bool = True) -> bytes:
+    """A FASTA query as the search kernels take it: SEG (unless disabled),
+    then the internal alphabet (run_seg + seq_2internal)."""
+    from . import alphabet as ab
+    if seg:
+        residues = seg_mask(residues)
+    return ab.aa_to_internal(np.frombuffer(residues, np.uint8)).tobytes()

@@ -262,3 +262,37 @@ def write_fasta(path: str, prot: Proteins, width: int = 60):
             b = s.tobytes()
             for i in range(0, len(b), width):
                 f.write(b[i:i + width] + b"\n")
+
+
+def protein_db_arrays(n: int, seed: int = 0, median=300, lo=50, hi=2000):
+    """(residues uint8 AA letters concatenated, lengths int64) of an n-protein
+    DB, drawn like protein_db but without per-protein arrays."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lens = lognormal_lengths(rng, n, median, lo, hi)
+    return random_residues(rng, int(lens.sum())), lens
+
+
+def search_queries_arrays(res: np.ndarray, lens: np.ndarray, n_mut: int, n_rand: int,
+                          seed: int = 2, identity=(0.30, 0.90), lo=50, hi=1500):
+    """Queries for the full-search configs: n_mut mutated from random DB
+    proteins (identity uniform in `identity`, indels at 0.02), n_rand random,
+    lengths clipped to [lo, hi].  Returns (residues, lengths)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    off = np.cumsum(lens) - lens
+    pick = rng.integers(0, len(lens), n_mut)
+    src = res[_segment_positions(off[pick], lens[pick])]
+    mres, mlen = mutate_batch(rng, src, lens[pick], rng.uniform(*identity, size=n_mut))
+    rlen = lognormal_lengths(rng, n_rand, 300, lo, hi)
+    rres = random_residues(rng, int(rlen.sum()))
+    # clip / pad the mutated ones to [lo, hi]
+    moff = np.cumsum(mlen) - mlen
+    keep = np.minimum(mlen, hi)
+    parts, plens = [], []
+    for o, k in zip(moff, keep):
+        s = mres[o:o + k]
+        if len(s) < lo:
+            s = np.concatenate([s, random_residues(rng, lo - len(s))])
+        parts.append(s)
+        plens.append(len(s))
+    allres = np.concatenate(parts + [rres])
+    return allres, np.concatenate([np.array(plens, np.int64), rlen])
