@@ -63,12 +63,17 @@ constexpr int kPadScore = -64;      // profile value of pad rows / pad columns
 constexpr int kMatStride = 32;      // shared matrix row stride (bytes)
 constexpr int kSmatBytes = 26 * kMatStride;
 
-// bytes per lane block of the profile: 4*W with W odd (bank-conflict free)
-__host__ __device__ constexpr int words_for(int R) {
-    return ((R + 3) / 4) % 2 == 1 ? (R + 3) / 4 : (R + 3) / 4 + 1;
-}
+// profile words per lane and pair: 4 rows per word
+__host__ __device__ constexpr int words_for(int R) { return (R + 3) / 4; }
 __host__ __device__ constexpr int profile_bytes(int R) { return 26 * 32 * 4 * words_for(R); }
-__host__ __device__ constexpr int smem_bytes(int R) { return kSmatBytes + 2 * profile_bytes(R); }
+constexpr int kRing = 128;          // subject-letter ring per warp (uint16 letter pairs)
+__host__ __device__ constexpr int smem_bytes(int R) {
+    return kSmatBytes + 2 * profile_bytes(R) + 2 * kRing;
+}
+// Fm "cleared" at an SSW lane start: any value <= 0 acts like the cleared
+// one there, so the start row adds -kBig instead of masking (exact while
+// every score stays below kBig; larger scores take the 32-bit rerun).
+constexpr int kBig = 32512;
 
 struct Args {
     const int8_t *q;
@@ -107,10 +112,28 @@ __device__ __forceinline__ uint64_t best_key(int v, int col, int row) {
                  : 0ull;
 }
 
-template <int R>
+// letter pair (A low byte, B high byte) of subject column c; past a
+// subject's end, and for bytes outside the alphabet, the pad letter
+__device__ __forceinline__ uint32_t letter_pair(const Args &a, const int8_t *sA, int slA,
+                                                const int8_t *sB, int slB, int c) {
+    int la = kPadLetter, lb = kPadLetter;
+    if (c < slA) {
+        la = sA[c];
+        if (a.translate) la = a.xs[la & 127];
+        if ((unsigned)la >= 25u) la = kPadLetter;
+    }
+    if (c < slB) {
+        lb = sB[c];
+        if (a.translate) lb = a.xs[lb & 127];
+        if ((unsigned)lb >= 25u) lb = kPadLetter;
+    }
+    return (uint32_t)la | ((uint32_t)lb << 8);
+}
+
+template <int R, bool MULTI>
 __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
-                                         uint32_t *profA, uint32_t *profB, int stripes,
-                                         uint32_t *bnd) {
+                                         uint32_t *profA, uint32_t *profB, uint16_t *ring,
+                                         int stripes, uint32_t *bnd) {
     constexpr int W = words_for(R);
     const int lane = threadIdx.x & 31;
 
@@ -137,10 +160,12 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     // stripe; the last row of a stripe (H, F, Fm per column) goes to `bnd`
     // and enters the next stripe at lane 0.  Lane 0 reads column k at step k
     // and lane 31 writes column k-31 at step k, so one buffer serves as both.
-    for (int st = 0; st < stripes; ++st) {
+    const int nstripes = MULTI ? stripes : 1;
+    for (int st = 0; st < nstripes; ++st) {
     const int i0 = (st * 32 + lane) * R;
 
-    // ---- profile of this lane's rows for all 26 letters (25 + pad column)
+    // ---- profile of this lane's rows for all 26 letters (25 + pad column),
+    // word w of letter l at [(l * W + w) * 32 + lane]: conflict-free per lane
     int qa[R], qb[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -150,6 +175,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             if (qa[r] >= 0) qa[r] = a.xq[qa[r] & 127];
             if (qb[r] >= 0) qb[r] = a.xq[qb[r] & 127];
         }
+        if (qa[r] >= 25) qa[r] = -1;
+        if (qb[r] >= 25) qb[r] = -1;
     }
     __syncwarp();
     for (int let = 0; let < 26; ++let) {
@@ -168,83 +195,101 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
                 wa |= (uint32_t)(uint8_t)(int8_t)va << (8 * k);
                 wb |= (uint32_t)(uint8_t)(int8_t)vb << (8 * k);
             }
-            profA[(let * 32 + lane) * W + w] = wa;
-            profB[(let * 32 + lane) * W + w] = wb;
+            profA[(let * W + w) * 32 + lane] = wa;
+            profB[(let * W + w) * 32 + lane] = wb;
         }
     }
+    // ---- subject letters: columns 0..63 in the ring, 64..95 in flight;
+    // every 32 steps the lanes store the next 32 columns and fetch 32 more
+    ring[lane] = (uint16_t)letter_pair(a, sA, slA, sB, slB, lane);
+    ring[32 + lane] = (uint16_t)letter_pair(a, sA, slA, sB, slB, 32 + lane);
+    ring[64 + lane] = (uint16_t)(kPadLetter | (kPadLetter << 8));
+    ring[96 + lane] = (uint16_t)(kPadLetter | (kPadLetter << 8));
+    uint32_t pre = letter_pair(a, sA, slA, sB, slB, 64 + lane);
     __syncwarp();
 
-    // ---- SSW lane starts of this lane's rows -> per-row clear masks for Fm
-    uint32_t mask[R];
+    // ---- SSW lane starts: the Fm terms of a start row add -kBig
+    uint32_t ngo[R], nge[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        uint32_t m = 0xFFFFFFFFu;
-        if ((i0 + r) % segA == 0) m &= 0xFFFF0000u;
-        if ((i0 + r) % segB == 0) m &= 0x0000FFFFu;
-        mask[r] = m;
+        const bool sa = (i0 + r) % segA == 0, sb = (i0 + r) % segB == 0;
+        ngo[r] = pack2(sa ? -kBig : -a.gap_open, sb ? -kBig : -a.gap_open);
+        nge[r] = pack2(sa ? -kBig : -a.gap_extend, sb ? -kBig : -a.gap_extend);
     }
 
     uint32_t E[R], H[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) { E[r] = 0u; H[r] = 0u; }
 
-    uint32_t outH = 0u, outF = 0u, outFm = 0u, outLet = 0u;
+    uint32_t outH = 0u, outF = 0u, outFm = 0u;
     uint32_t diag = 0u;
     uint32_t runmax = 0u;
     int colA = -1, rowA = 0, colB = -1, rowB = 0;
 
+    // profile words of this step's column (j = k - lane), fetched one step
+    // ahead; the letter pair of the column after it
+    uint32_t wa[W], wb[W];
+    {
+        const uint32_t l = ring[(-lane) & (kRing - 1)];
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            wa[w] = profA[((l & 0xFFu) * W + w) * 32 + lane];
+            wb[w] = profB[((l >> 8) * W + w) * 32 + lane];
+        }
+    }
+    uint32_t let1 = ring[(1 - lane) & (kRing - 1)];
 
     const int steps = N + 31;
     for (int k = 0; k < steps; ++k) {
+        const int j = k - lane;
+        if ((k & 31) == 0 && k > 0) {
+            ring[(k + 32 + lane) & (kRing - 1)] = (uint16_t)pre;
+            pre = letter_pair(a, sA, slA, sB, slB, k + 64 + lane);
+            __syncwarp();
+        }
         uint32_t inH = __shfl_up_sync(0xFFFFFFFFu, outH, 1);
         uint32_t inF = __shfl_up_sync(0xFFFFFFFFu, outF, 1);
         uint32_t inFm = __shfl_up_sync(0xFFFFFFFFu, outFm, 1);
-        uint32_t inLet = __shfl_up_sync(0xFFFFFFFFu, outLet, 1);
         if (lane == 0) {
-            if (st == 0 || k >= N) {
-                inH = 0u; inF = 0u; inFm = 0u;
-            } else {
+            if (MULTI && st > 0 && k < N) {
                 const uint32_t *b = bnd + 3 * (size_t)k;
                 inH = b[0]; inF = b[1]; inFm = b[2];
+            } else {
+                inH = 0u; inF = 0u; inFm = 0u;
             }
-            // the subject letters of column k enter at lane 0 (an L1-resident
-            // byte load; cheaper here than a shuffle-fed prefetch window)
-            int la = k < slA ? sA[k] : kPadLetter;
-            int lb = k < slB ? sB[k] : kPadLetter;
-            if (a.translate) {
-                if (k < slA) la = a.xs[la & 127];
-                if (k < slB) lb = a.xs[lb & 127];
-            }
-            inLet = (uint32_t)la | ((uint32_t)lb << 8);
         }
-        const int j = k - lane;
-        if (j >= 0 && j < N) {
-            const uint32_t *pa = profA + ((inLet & 0xFFu) * 32 + lane) * W;
-            const uint32_t *pb = profB + ((inLet >> 8) * 32 + lane) * W;
-            uint32_t wa[W], wb[W];
+        // next step's profile words
+        uint32_t na[W], nb[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) { wa[w] = pa[w]; wb[w] = pb[w]; }
-            uint32_t F = inF, Fm = inFm, D = diag, cm = 0u;
+        for (int w = 0; w < W; ++w) {
+            na[w] = profA[((let1 & 0xFFu) * W + w) * 32 + lane];
+            nb[w] = profB[((let1 >> 8) * W + w) * 32 + lane];
+        }
+        let1 = ring[(j + 2) & (kRing - 1)];
+        if (j >= 0 && j < N) {
+            uint32_t F = inF, Fm = inFm, D = diag;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const uint32_t sc = prmt(wa[r >> 2], wb[r >> 2], SEL[r & 3]);
-                Fm &= mask[r];
                 const uint32_t X = __viaddmax_s16x2_relu(D, sc, E[r]);
                 const uint32_t Hn = __vimax_s16x2_relu(X, F);
                 const uint32_t Xg = __viaddmax_s16x2(X, NGO, NEGINF);
-                const uint32_t Gp = __viaddmax_s16x2(Fm, NGO, Xg);
+                const uint32_t Gp = __viaddmax_s16x2(Fm, ngo[r], Xg);
                 E[r] = __viaddmax_s16x2(E[r], NGE, Gp);
                 F = __viaddmax_s16x2(F, NGE, Xg);
-                Fm = __viaddmax_s16x2(Fm, NGE, Xg);
+                Fm = __viaddmax_s16x2(Fm, nge[r], Xg);
                 D = H[r];
                 H[r] = Hn;
-                cm = __vimax_s16x2_relu(cm, Hn);
             }
+            // column maximum of the lane's rows (all H >= 0)
+            uint32_t cm = H[0];
+#pragma unroll
+            for (int r = 1; r + 1 < R; r += 2) cm = __vimax3_s16x2(cm, H[r], H[r + 1]);
+            if ((R & 1) == 0) cm = __vimax_s16x2_relu(cm, H[R - 1]);
             outH = H[R - 1];
             outF = F;
             outFm = Fm;
-            outLet = inLet;
-            if (lane == 31 && st + 1 < stripes) {
+            if (MULTI && lane == 31 && st + 1 < stripes) {
                 uint32_t *b = bnd + 3 * (size_t)j;
                 b[0] = outH; b[1] = outF; b[2] = outFm;
             }
@@ -270,6 +315,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             }
         }
         diag = inH;
+#pragma unroll
+        for (int w = 0; w < W; ++w) { wa[w] = na[w]; wb[w] = nb[w]; }
     }
 
     kA = max(kA, best_key(lo16(runmax), colA, rowA));
@@ -315,6 +362,7 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
     int8_t *smat = reinterpret_cast<int8_t *>(smem);
     uint32_t *profA = reinterpret_cast<uint32_t *>(smem + kSmatBytes);
     uint32_t *profB = profA + profile_bytes(R) / 4;
+    uint16_t *ring = reinterpret_cast<uint16_t *>(profB + profile_bytes(R) / 4);
     const int lane = threadIdx.x;
     const int start = a.rinfo[2 * bin];
     const int count = a.rinfo[2 * bin + 1];
@@ -333,8 +381,14 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
         if (t >= ntask) break;
         const int pA = a.sorted[start + 2 * t];
         const int pB = 2 * t + 1 < count ? a.sorted[start + 2 * t + 1] : -1;
-        run_task<R>(a, pA, pB, smat, profA, profB, stripes,
-                    a.bnd ? a.bnd + (size_t)blockIdx.x * a.bnd_words : nullptr);
+        if constexpr (R == kMaxR) {
+            if (stripes > 1) {
+                run_task<R, true>(a, pA, pB, smat, profA, profB, ring, stripes,
+                                  a.bnd + (size_t)blockIdx.x * a.bnd_words);
+                continue;
+            }
+        }
+        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr);
     }
 }
 
@@ -657,7 +711,7 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     a.bnd_words = 0;
     a.exact_list = exact_list;
     a.exact_count = exact_count;
-    a.exact_threshold = 32767 - 2 * std::max(mx, 1);
+    a.exact_threshold = std::min(32767 - 2 * std::max(mx, 1), kBig);
 
     int64_t launches = 0;
     int host_maxn = 0;
@@ -669,8 +723,9 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     a.ssw_lanes = 8;
     rc = launch_round(cfg, a, n, rerun, rerun_count, counts, cursor, sorted, multi_maxn, st,
                       launches, nullptr);
-    if (rc == TPZ_OK && host_maxn > 0) {
-        // only queries longer than one stripe can come near 32767
+    if (rc == TPZ_OK && (host_maxn > 0 || (int64_t)kStripeRows * mx >= a.exact_threshold)) {
+        // only queries longer than one stripe, or matrices with large
+        // entries, can come near the 16-bit limit
         int32_t *scratch = nullptr;
         rc = cudaMallocAsync((void **)&scratch,
                              sizeof(int32_t) * 2 * (size_t)TPZ_SW_MAX_QLEN * kExactThreads, st)
