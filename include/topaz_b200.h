@@ -156,8 +156,9 @@ TPZ_API int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_
  * query_perform_alignments (src/query.c:94-248) for a batch of queries
  * (internal alphabet, as after run_seg + seq_2internal, src/engine.c:250-277).
  * Hits come back per query in hitlist traversal order (gapless score
- * descending, newest first; src/rbtree.c:653-669).  E-values and ranking are
- * done by the caller (tpz_karlin, output_top_hits).
+ * descending, newest first; src/rbtree.c:653-669) with E-values and ranking
+ * left to the caller (tpz_karlin, output_top_hits), or, in report mode,
+ * ranked and cut on the device.
  * ------------------------------------------------------------------------ */
 #define TPZ_SEARCH_MAX_QLEN 8192
 
@@ -170,6 +171,18 @@ typedef struct {
     int32_t alignments;       /* -A: hitlist capacity */
     const int8_t *mat625;     /* substitution matrix (host) */
     int64_t trace_pops;       /* record up to this many pops per query (0: none) */
+    /* Report mode (report_hits > 0): the ranking of output_top_hits
+     * (src/engine.c:193-248) on the device.  Each query's aligned hits (SW
+     * score, or gapless score < 40 with bitscore 0 and E-value 1000) are
+     * stably sorted by bitscore descending, the first report_hits are kept and
+     * those with E-value > max_evalue dropped; only these come back, in that
+     * order, with bitscore and E-value.  Scores use tpz_karlin with the
+     * parameters below (src/ssw_wrapper.c:179-183).  0: every hit comes back
+     * in traversal order without E-values. */
+    int32_t report_hits;      /* -H */
+    double max_evalue;        /* -E */
+    double lambda, k, H;      /* Karlin-Altschul parameters (0.267, 0.041, 0.140) */
+    uint64_t db_size, db_proteins;
 } tpz_search_opts;
 
 typedef struct {
@@ -182,8 +195,10 @@ typedef struct {
     const int64_t *trace_n;                  /* nq (when trace_pops > 0) */
     const int64_t *trace_row;                /* nq * trace_pops */
     const int32_t *trace_off, *trace_score, *trace_len, *trace_counted;
-    double stage_ms[4];      /* device time: seed lookup, walk + hitlist, SW of hits;
-                                [3] = host wall time of the whole call incl. copies */
+    double stage_ms[4];      /* device time: seed lookup, walk + hitlist, SW of hits
+                                (+ ranking in report mode); [3] = host wall time of
+                                the whole call incl. copies */
+    const double *bitscore, *evalue;         /* per hit, report mode only (else NULL) */
 } tpz_search_result;
 
 TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,

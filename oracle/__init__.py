@@ -138,3 +138,14 @@ def oracle_query(db, qint: bytes, mat, opts: Opts, max_pops=1 << 20, max_hits=81
     pops = {"row": rows[:n], "off": arr[0][:n], "score": arr[1][:n], "len": arr[2][:n],
             "counted": arr[3][:n]}
     return pops, list(hits[:max(nh, 0)]), npops.value, ncnt.value, nh
+
+
+def oracle_rank_select(hits, num_hits, evalue):
+    """Indices into `hits` (traversal order) of the lines output_top_hits
+    prints, in print order."""
+    L = liboracle()
+    arr = (OHit * max(len(hits), 1))(*hits)
+    out = np.zeros(max(len(hits), 1), np.int32)
+    k = L.orc_rank_select(arr, ctypes.c_int32(len(hits)), ctypes.c_int32(num_hits),
+                          ctypes.c_double(evalue), _p(out))
+    return [int(i) for i in out[:k]]

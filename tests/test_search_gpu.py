@@ -92,6 +92,35 @@ def test_search_matches_oracle(cuda, fresh, seeds, aligns):
                     assert (r["rawscore"][k], r["qend"][k], r["send"][k]) == (h.rawscore, h.qend, h.send)
 
 
+@pytest.mark.parametrize("num_hits,evalue,k", [(100, 1e-3, 0.041), (7, 10.0, 0.041),
+                                                (400, 2000.0, 0.041), (1, 1e-30, 0.041),
+                                                (50, 1e6, 2.0)])
+def test_search_report_mode_matches_oracle_ranking(cuda, fresh, num_hits, evalue, k):
+    """Device ranking, -H cut and E-value cut (report mode) against the
+    oracle's output_top_hits selection; k = 2 puts low scores below the
+    bitscore-0 gapless hits, so those interleave with aligned hits."""
+    db, qs = fresh
+    ix = native.Index(db)
+    r = ix.search(qs, BLOSUM62, num_hits=num_hits, report={"max_evalue": evalue, "k": k})
+    opts = oracle.Opts(num_hits, evalue, 11, 1, 0.267, k, 0.14, 5, 300000, 5000)
+    nsel = 0
+    for q, qi in enumerate(qs):
+        _, hits, _, _, nh = oracle.oracle_query(db, qi, BLOSUM62, opts)
+        assert nh >= 0
+        sel = oracle.oracle_rank_select(hits, num_hits, evalue)
+        a, b = r["hit_off"][q], r["hit_off"][q + 1]
+        assert b - a == len(sel)
+        nsel += len(sel)
+        assert list(r["protein"][a:b]) == [hits[i].db_index for i in sel]
+        assert list(r["bitscore"][a:b]) == [hits[i].bitscore for i in sel]
+        assert list(r["evalue"][a:b]) == [hits[i].evalue for i in sel]
+        sw = r["sw_status"][a:b] == native.TPZ_SW_OK
+        assert list(r["rawscore"][a:b][sw]) == [hits[i].rawscore for i, s in zip(sel, sw) if s]
+        assert list(r["qend"][a:b][sw]) == [hits[i].qend for i, s in zip(sel, sw) if s]
+        assert list(r["send"][a:b][sw]) == [hits[i].send for i, s in zip(sel, sw) if s]
+    assert nsel > 0
+
+
 def test_sa_search_and_hsp_stage_entry_points(cuda, fresh):
     db, qs = fresh
     ix = native.Index(db)

@@ -127,17 +127,277 @@ __global__ void scatter_sw_kernel(int64_t n, const int32_t *p_hit, const int32_t
     }
 }
 
+// ---- report mode: output_top_hits (src/engine.c:193-248) on the device
+
+constexpr int kRawRanks = 32768;      // SW scores 0..32766 (32767 is dropped)
+constexpr int kRankThreads = 512;
+constexpr int kRankSmemKeys = 16384;  // sort buffer in shared memory up to this size
+
+struct RankArgs {
+    const int64_t *hit_off;           // nq + 1
+    const int32_t *raw, *sw_status;
+    const int32_t *rank_of_raw;       // kRawRanks: dense rank of each score's bitscore
+    int32_t rank_low;                 // rank of bitscore 0 (gapless score < 40)
+    int low_last;                     // every SW score ranks above bitscore 0
+    int low_pass;                     // E-value 1000 passes the cut
+    const int32_t *rank_min;          // nq: lowest rank whose E-value passes
+    int nq, top, npad;
+    uint64_t *gbuf;                   // nq * npad, when the buffer is not in shared memory
+    int32_t *sel, *nsel;              // nq * top hit indices in rank order; counts
+};
+
+// sort key: bitscore rank descending, then traversal index ascending (the
+// stable merge sort of the reference's qsort); bit 0 marks gapless-low hits
+__device__ __forceinline__ uint64_t rank_key(int rank, int i, int low) {
+    return ((uint64_t)(rank + 1) << 40) | ((uint64_t)(0x7FFFFFFF - i) << 1) | (uint64_t)low;
+}
+
+// One block per query: sort the query's aligned hits, keep the first `top`,
+// drop those over the E-value cut.
+__global__ void __launch_bounds__(kRankThreads) rank_select_kernel(RankArgs a) {
+    extern __shared__ uint64_t sbuf[];
+    __shared__ int cnt;
+    const int q = blockIdx.x;
+    uint64_t *buf = a.gbuf ? a.gbuf + (size_t)q * a.npad : sbuf;
+    const int64_t base = a.hit_off[q];
+    const int n = (int)(a.hit_off[q + 1] - base);
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int st = a.sw_status[base + i];
+        uint64_t key = 0;
+        if (st == TPZ_SW_OK) key = rank_key(a.rank_of_raw[a.raw[base + i]], i, 0);
+        else if (st == TPZ_SW_GAPLESS_LOW && !a.low_last) key = rank_key(a.rank_low, i, 1);
+        if (key) buf[atomicAdd(&cnt, 1)] = key;
+    }
+    __syncthreads();
+    const int m = cnt;
+    int p = 1;
+    while (p < m) p <<= 1;
+    for (int i = m + threadIdx.x; i < p; i += blockDim.x) buf[i] = 0;
+    __syncthreads();
+    // bitonic sort, descending (keys are distinct; padding 0 sorts last)
+    for (int k = 2; k <= p; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < p; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const uint64_t x = buf[i], y = buf[l];
+                    if (((i & k) == 0) ? (x < y) : (x > y)) { buf[i] = y; buf[l] = x; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        int32_t *out = a.sel + (int64_t)q * a.top;
+        int ns = 0;
+        const int take = min(m, a.top);
+        for (int t = 0; t < take; ++t) {
+            const uint64_t key = buf[t];
+            const int i = 0x7FFFFFFF - (int)((key >> 1) & 0x7FFFFFFF);
+            const int rank = (int)(key >> 40) - 1;
+            const bool pass = (key & 1) ? a.low_pass != 0 : rank >= a.rank_min[q];
+            if (pass) out[ns++] = (int32_t)(base + i);
+        }
+        if (a.low_last && a.low_pass) {
+            // gapless-low hits rank after every aligned hit, in traversal order
+            int room = a.top - take;
+            for (int i = 0; i < n && room > 0; ++i)
+                if (a.sw_status[base + i] == TPZ_SW_GAPLESS_LOW) { out[ns++] = (int32_t)(base + i); --room; }
+        }
+        a.nsel[q] = ns;
+    }
+}
+
+// exclusive prefix sum of n counts into off[0..n] (one block of 1024)
+__global__ void __launch_bounds__(1024) offsets_kernel(const int32_t *cnt, int n, int64_t *off) {
+    __shared__ int64_t part[1024];
+    __shared__ int64_t carry;
+    const int t = threadIdx.x;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (int b = 0; b < n; b += 1024) {
+        const int i = b + t;
+        const int64_t v = i < n ? cnt[i] : 0;
+        part[t] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            const int64_t x = t >= o ? part[t - o] : 0;
+            __syncthreads();
+            part[t] += x;
+            __syncthreads();
+        }
+        if (i < n) off[i] = carry + part[t] - v;
+        __syncthreads();
+        if (t == 1023) carry += part[1023];
+        __syncthreads();
+    }
+    if (t == 0) off[n] = carry;
+}
+
+constexpr int kGatherFields = 8;
+struct GatherArgs {
+    const int32_t *sel, *nsel;
+    const int64_t *off;
+    int nq, top;
+    const int32_t *src[kGatherFields];
+    int32_t *dst[kGatherFields];
+};
+
+__global__ void gather_selected_kernel(GatherArgs g) {
+    const int64_t total = (int64_t)g.nq * g.top;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total;
+         x += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(x / g.top), k = (int)(x % g.top);
+        if (k >= g.nsel[q]) continue;
+        const int h = g.sel[x];
+        const int64_t d = g.off[q] + k;
+#pragma unroll
+        for (int f = 0; f < kGatherFields; ++f) g.dst[f][d] = g.src[f][h];
+    }
+}
+
 struct ResultHolder {
     tpz_search_result r{};
     std::vector<int64_t> hit_off, npops, ncounted, trace_n, trace_row;
     std::vector<int32_t> status, protein, gs, gl, so, raw, qend, send, sw_status;
     std::vector<int32_t> trace_off, trace_score, trace_len, trace_counted;
+    std::vector<double> bits, evalue;
 };
+
+// Ranking tables of report mode.  The bitscore of a raw score does not
+// depend on the query (src/ssw_wrapper.c:179-182), so sorting hits by
+// bitscore is sorting them by the dense rank of their score's bitscore; the
+// E-value cut of a query is a lowest passing rank, found by bisection since
+// the E-value does not increase with the bitscore.
+struct RankTables {
+    std::vector<int32_t> rank_of_raw;   // kRawRanks
+    int32_t rank_low = 0;
+    int low_last = 0, low_pass = 0;
+    std::vector<int32_t> reps, rep_raw; // ranks held by some raw score (ascending), one raw each
+};
+
+int rank_tables(const tpz_search_opts *o, RankTables *t) {
+    std::vector<double> b(kRawRanks);
+    double ev;
+    for (int r = 0; r < kRawRanks; ++r) {
+        tpz_karlin(1, 1, 1, o->lambda, o->k, o->H, r, &b[r], &ev);
+        if (b[r] != b[r]) { tpz::set_error("tpz_search_batch: bitscores are NaN (check lambda, k)"); return TPZ_E_ARG; }
+        // two scores sharing a bitscore must share the E-value too (the cut
+        // is taken per rank)
+        if (r > 0 && b[r] == b[r - 1] && o->lambda * r - log(o->k) != o->lambda * (r - 1) - log(o->k)) {
+            tpz::set_error("tpz_search_batch: lambda too small to rank scores by bitscore");
+            return TPZ_E_ARG;
+        }
+    }
+    std::vector<double> u(b);
+    u.push_back(0.0);
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    auto rank = [&](double v) { return (int32_t)(std::lower_bound(u.begin(), u.end(), v) - u.begin()); };
+    t->rank_of_raw.resize(kRawRanks);
+    std::vector<int32_t> rep(u.size(), -1);
+    int32_t minr = INT32_MAX;
+    for (int r = 0; r < kRawRanks; ++r) {
+        const int32_t k = rank(b[r]);
+        t->rank_of_raw[r] = k;
+        if (rep[k] < 0) rep[k] = r;
+        minr = std::min(minr, k);
+    }
+    for (size_t k = 0; k < rep.size(); ++k)
+        if (rep[k] >= 0) { t->reps.push_back((int32_t)k); t->rep_raw.push_back(rep[k]); }
+    t->rank_low = rank(0.0);
+    t->low_last = t->rank_low < minr;
+    t->low_pass = 1000.0 <= o->max_evalue;
+    return TPZ_OK;
+}
+
+// lowest rank whose E-value passes for a query of length qlen (INT32_MAX: none)
+int32_t rank_min_for(const RankTables &t, const tpz_search_opts *o, int32_t qlen) {
+    int64_t lo = 0, hi = (int64_t)t.reps.size();
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        double bits, ev;
+        tpz_karlin(qlen, o->db_size, o->db_proteins, o->lambda, o->k, o->H,
+                   t.rep_raw[mid], &bits, &ev);
+        if (ev <= o->max_evalue) hi = mid; else lo = mid + 1;
+    }
+    return lo < (int64_t)t.reps.size() ? t.reps[lo] : INT32_MAX;
+}
 
 bool letters_ok(const char *s, int64_t n) {
     for (int64_t i = 0; i < n; ++i)
         if (s[i] < 'A' || s[i] > 'Y') return false;
     return true;
+}
+
+// Report mode after the SW of a batch: rank, select and gather on the device,
+// then copy the reported hits and score them with tpz_karlin.
+int report_select(DevBuf &b, ResultHolder *R, int64_t nq, int64_t maxq, const int32_t *qlen,
+                  const tpz_search_opts *o, const RankTables &rt, int64_t nh, int32_t *pprot,
+                  int32_t *pgs, int32_t *pgl, int32_t *pso, int32_t *raw, int32_t *qend,
+                  int32_t *send, int32_t *psw, cudaEvent_t done) {
+    const int top = o->report_hits;
+    int npad = 1;
+    while (npad < maxq) npad <<= 1;
+    std::vector<int32_t> rmin(nq);
+    for (int64_t q = 0; q < nq; ++q) rmin[q] = rank_min_for(rt, o, qlen[q]);
+    int32_t *d_rank, *d_rmin, *d_sel, *d_nsel; int64_t *d_off, *d_hoff; uint64_t *d_gbuf = nullptr;
+    int32_t *dst[kGatherFields];
+    int rc;
+    if ((rc = b.alloc(&d_rank, kRawRanks)) || (rc = b.alloc(&d_rmin, nq)) ||
+        (rc = b.alloc(&d_sel, (size_t)nq * top)) || (rc = b.alloc(&d_nsel, nq)) ||
+        (rc = b.alloc(&d_off, nq + 1)) || (rc = b.alloc(&d_hoff, nq + 1)))
+        return rc;
+    for (int f = 0; f < kGatherFields; ++f)
+        if ((rc = b.alloc(&dst[f], (size_t)std::min<int64_t>(nh, nq * (int64_t)top)))) return rc;
+    const bool in_smem = npad <= kRankSmemKeys;
+    if (!in_smem && (rc = b.alloc(&d_gbuf, (size_t)nq * npad))) return rc;
+    TPZ_CUDA(cudaMemcpy(d_rank, rt.rank_of_raw.data(), 4 * kRawRanks, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(d_rmin, rmin.data(), 4 * nq, cudaMemcpyHostToDevice));
+    TPZ_CUDA(cudaMemcpy(d_hoff, R->hit_off.data(), 8 * (nq + 1), cudaMemcpyHostToDevice));
+    RankArgs ra;
+    ra.hit_off = d_hoff; ra.raw = raw; ra.sw_status = psw; ra.rank_of_raw = d_rank;
+    ra.rank_low = rt.rank_low; ra.low_last = rt.low_last; ra.low_pass = rt.low_pass;
+    ra.rank_min = d_rmin; ra.nq = (int)nq; ra.top = top; ra.npad = npad; ra.gbuf = d_gbuf;
+    ra.sel = d_sel; ra.nsel = d_nsel;
+    const size_t smem = in_smem ? sizeof(uint64_t) * npad : 0;
+    if (smem > 48 * 1024)
+        TPZ_CUDA(cudaFuncSetAttribute((const void *)rank_select_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rank_select_kernel<<<(unsigned)nq, kRankThreads, smem>>>(ra);
+    offsets_kernel<<<1, 1024>>>(d_nsel, (int)nq, d_off);
+    GatherArgs g;
+    g.sel = d_sel; g.nsel = d_nsel; g.off = d_off; g.nq = (int)nq; g.top = top;
+    const int32_t *src[kGatherFields] = {pprot, pgs, pgl, pso, raw, qend, send, psw};
+    for (int f = 0; f < kGatherFields; ++f) { g.src[f] = src[f]; g.dst[f] = dst[f]; }
+    const int64_t tot = nq * (int64_t)top;
+    gather_selected_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256>>>(g);
+    TPZ_CUDA(cudaGetLastError());
+    TPZ_CUDA(cudaEventRecord(done, 0));
+    R->hit_off.assign(nq + 1, 0);
+    TPZ_CUDA(cudaMemcpy(R->hit_off.data(), d_off, 8 * (nq + 1), cudaMemcpyDeviceToHost));
+    const int64_t n = R->hit_off[nq];
+    std::vector<int32_t> *host[kGatherFields] = {&R->protein, &R->gs, &R->gl, &R->so,
+                                                 &R->raw, &R->qend, &R->send, &R->sw_status};
+    for (int f = 0; f < kGatherFields; ++f) {
+        host[f]->resize(n);
+        if (n) TPZ_CUDA(cudaMemcpy(host[f]->data(), dst[f], 4 * n, cudaMemcpyDeviceToHost));
+    }
+    R->bits.resize(n);
+    R->evalue.resize(n);
+    for (int64_t q = 0; q < nq; ++q)
+        for (int64_t h = R->hit_off[q]; h < R->hit_off[q + 1]; ++h) {
+            if (R->sw_status[h] == TPZ_SW_OK) {
+                tpz_karlin(qlen[q], o->db_size, o->db_proteins, o->lambda, o->k, o->H, R->raw[h],
+                           &R->bits[h], &R->evalue[h]);
+            } else {
+                R->bits[h] = 0;
+                R->evalue[h] = 1000;
+            }
+        }
+    return TPZ_OK;
 }
 
 }  // namespace
@@ -328,6 +588,16 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
                        "min_hit_length/seeds/alignments/num_hits >= 1)");
         return TPZ_E_ARG;
     }
+    const bool report = o->report_hits > 0;
+    RankTables rt;
+    if (report) {
+        if (!(o->k > 0) || o->max_evalue != o->max_evalue) {
+            tpz::set_error("tpz_search_batch: report mode needs k > 0 and a max_evalue");
+            return TPZ_E_ARG;
+        }
+        const int rc0 = rank_tables(o, &rt);
+        if (rc0) return rc0;
+    }
     int maxm = 0;
     for (int i = 0; i < 625; ++i) maxm = std::max<int>(maxm, o->mat625[i]);
     if (255 * maxm >= kSMax) { tpz::set_error("tpz_search_batch: matrix entries too large"); return TPZ_E_ARG; }
@@ -424,8 +694,11 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         R->status[q] = qo[q].status | qstatus[q];
     }
     const int64_t nh = R->hit_off[nq];
-    for (auto *v : {&R->protein, &R->gs, &R->gl, &R->so, &R->raw, &R->qend, &R->send, &R->sw_status})
-        v->assign(nh, -1);
+    if (!report)
+        for (auto *v : {&R->protein, &R->gs, &R->gl, &R->so, &R->raw, &R->qend, &R->send, &R->sw_status})
+            v->assign(nh, -1);
+    int64_t maxq = 0;
+    for (int64_t q = 0; q < nq; ++q) maxq = std::max<int64_t>(maxq, qo[q].nhits);
 
     if (nh > 0) {
         int64_t *dho, *pq_off, *ps_off; int32_t *pprot, *pgs, *pgl, *pso, *psw, *pq_len, *ps_len, *p_hit, *dnp;
@@ -460,6 +733,11 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
             scatter_sw_kernel<<<(unsigned)std::min<int64_t>((npairs + 255) / 256, 4096), 256>>>(
                 npairs, p_hit, sc, re, rd, st, raw, send, qend, psw);
         }
+        if (report) {
+            int rc2 = report_select(b, R, nq, maxq, qlen, o, rt, nh, pprot, pgs, pgl, pso, raw, qend, send,
+                                    psw, ev[3]);
+            if (rc2) return bail(rc2);
+        } else {
         if (cudaEventRecord(ev[3], 0) != cudaSuccess)
             return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch event"));
         if (cudaMemcpy(R->protein.data(), pprot, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
@@ -471,6 +749,9 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
             cudaMemcpy(R->qend.data(), qend, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess ||
             cudaMemcpy(R->send.data(), send, 4 * nh, cudaMemcpyDeviceToHost) != cudaSuccess)
             return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch results"));
+        }
+    } else if (report) {
+        R->hit_off.assign(nq + 1, 0);
     }
     if (o->trace_pops > 0) {
         std::vector<PopRec> tr((size_t)nq * o->trace_pops);
@@ -497,6 +778,11 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     r.trace_score = o->trace_pops > 0 ? R->trace_score.data() : nullptr;
     r.trace_len = o->trace_pops > 0 ? R->trace_len.data() : nullptr;
     r.trace_counted = o->trace_pops > 0 ? R->trace_counted.data() : nullptr;
+    if (report) {
+        r.nhits_total = R->hit_off[nq];
+        r.bitscore = R->bits.data();
+        r.evalue = R->evalue.data();
+    }
     TPZ_CUDA(cudaDeviceSynchronize());
     float t01 = 0, t12 = 0, t23 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);

@@ -169,6 +169,18 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     so.seeds = o->number_of_seeds;
     so.alignments = o->number_of_alignments;
     so.mat625 = mat;
+    /* ranking and the E-value cut on the device (report mode) unless the
+     * Karlin parameters are outside what it takes (k <= 0, NaN -E) */
+    const int report = o->k > 0 && o->evalue == o->evalue;
+    if (report) {
+        so.report_hits = o->num_hits;
+        so.max_evalue = o->evalue;
+        so.lambda = o->lambda;
+        so.k = o->k;
+        so.H = o->H;
+        so.db_size = db_size;
+        so.db_proteins = db_proteins;
+    }
     while (!done) {
         int64_t nq = 0;
         tpzh_record r;
@@ -206,6 +218,12 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
                         qs[q].id_len, qs[q].id);
             const int64_t a = res->hit_off[q], b = res->hit_off[q + 1];
             int64_t n = 0;
+            if (report) {
+                /* already ranked, cut to -H and to -E */
+                for (int64_t h = a; h < b; ++h) {
+                    rk[n].idx = h; rk[n].bits = res->bitscore[h]; rk[n].evalue = res->evalue[h]; n++;
+                }
+            } else
             for (int64_t h = a; h < b; ++h) {
                 const int st = res->sw_status[h];
                 if (st == TPZ_SW_OK) {
@@ -217,8 +235,10 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
                     rk[n].idx = h; rk[n].bits = 0; rk[n].evalue = 1000; n++;
                 }
             }
-            stable_sort_bits(rk, n, tmp);
-            if (n > o->num_hits) n = o->num_hits;
+            if (!report) {
+                stable_sort_bits(rk, n, tmp);
+                if (n > o->num_hits) n = o->num_hits;
+            }
             int count = 0;
             int8_t *qidx = NULL;
             for (int64_t i = 0; i < n; ++i) {

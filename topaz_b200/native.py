@@ -125,7 +125,10 @@ class _SearchOpts(ctypes.Structure):
     _fields_ = [("num_hits", ctypes.c_int32), ("gap_open", ctypes.c_int32),
                 ("gap_extend", ctypes.c_int32), ("min_hit_length", ctypes.c_int32),
                 ("seeds", ctypes.c_int32), ("alignments", ctypes.c_int32),
-                ("mat625", _VP), ("trace_pops", ctypes.c_int64)]
+                ("mat625", _VP), ("trace_pops", ctypes.c_int64),
+                ("report_hits", ctypes.c_int32), ("max_evalue", ctypes.c_double),
+                ("lam", ctypes.c_double), ("k", ctypes.c_double), ("H", ctypes.c_double),
+                ("db_size", ctypes.c_uint64), ("db_proteins", ctypes.c_uint64)]
 
 
 _P64 = ctypes.POINTER(ctypes.c_int64)
@@ -139,7 +142,9 @@ class _SearchResult(ctypes.Structure):
                 ("suffix_offset", _P32), ("rawscore", _P32), ("qend", _P32), ("send", _P32),
                 ("sw_status", _P32), ("trace_n", _P64), ("trace_row", _P64),
                 ("trace_off", _P32), ("trace_score", _P32), ("trace_len", _P32),
-                ("trace_counted", _P32), ("stage_ms", ctypes.c_double * 4)]
+                ("trace_counted", _P32), ("stage_ms", ctypes.c_double * 4),
+                ("bitscore", ctypes.POINTER(ctypes.c_double)),
+                ("evalue", ctypes.POINTER(ctypes.c_double))]
 
 
 def _search_sigs(L):
@@ -222,16 +227,29 @@ class Index:
         return sc, ln
 
     def search(self, queries, mat, num_hits=100, gap_open=11, gap_extend=1, min_hit_length=5,
-               seeds=300000, alignments=5000, trace_pops=0):
+               seeds=300000, alignments=5000, trace_pops=0, report=None):
         """Runs a batch of queries (internal-alphabet bytes).  Returns a dict
         of numpy arrays (per query: hit_off, npops, ncounted, status; per hit:
         protein, gapless_score, gapless_length, suffix_offset, rawscore,
-        qend, send, sw_status; optional trace_*)."""
+        qend, send, sw_status; optional trace_*).
+
+        report: None for every hit in traversal order, or a dict with
+        max_evalue (and optionally hits, lam, k, H, db_size, db_proteins) for
+        the ranked, E-value-cut top hits with bitscore and evalue arrays."""
         L = lib()
         cat, off, lens = _concat(queries)
         mat = np.ascontiguousarray(mat, dtype=np.int8)
         o = _SearchOpts(num_hits, gap_open, gap_extend, min_hit_length, seeds, alignments,
                         _p(mat), trace_pops)
+        if report is not None:
+            T, P = len(self._T), len(self._ind)
+            o.report_hits = int(report.get("hits", num_hits))
+            o.max_evalue = float(report.get("max_evalue", 1e-3))
+            o.lam = float(report.get("lam", 0.267))
+            o.k = float(report.get("k", 0.041))
+            o.H = float(report.get("H", 0.140))
+            o.db_size = int(report.get("db_size", T - P))
+            o.db_proteins = int(report.get("db_proteins", P))
         res = ctypes.POINTER(_SearchResult)()
         check(L.tpz_search_batch(self.handle, _p(cat), _p(off), _p(lens), len(queries),
                                  ctypes.byref(o), ctypes.byref(res)))
@@ -248,6 +266,9 @@ class Index:
                       "qend", "send", "sw_status"):
                 out[k] = arr(getattr(r, k), nh)
             out["stage_ms"] = list(r.stage_ms)
+            if report is not None:
+                out["bitscore"] = arr(r.bitscore, nh)
+                out["evalue"] = arr(r.evalue, nh)
             if trace_pops:
                 out["trace_n"] = arr(r.trace_n, nq)
                 for k in ("trace_row", "trace_off", "trace_score", "trace_len", "trace_counted"):
