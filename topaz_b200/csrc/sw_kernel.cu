@@ -32,6 +32,14 @@
 // lane, so the 32 per-lane loads of a step never share a bank; prmt with the
 // sign-replicate selector widens two profile bytes into one int16x2 operand.
 //
+// End coordinates: each lane keeps the running maximum of its rows and the
+// column/row where it last rose.  A rise is only looked at when it reaches
+// the warp maximum of the last refresh (every 32 steps; a lower value cannot
+// be the alignment's maximum), and then the whole warp finds the first row
+// holding the new value with packed DPX ops, so the common case costs one
+// vote per step.  Steps run two at a time, the profile words ping-ponging
+// between two register sets.
+//
 // Pairs are binned on the device by R = ceil(qlen/32) and by subject length
 // (counting sort), paired two per task within a bin, and drained by one
 // persistent kernel per R from an atomic task counter.  Pairs whose u8-pass
@@ -53,7 +61,7 @@ namespace sw {
 
 constexpr int kMaxR = 32;           // rows per lane; one stripe = 32 lanes x R rows
 constexpr int kStripeRows = 32 * kMaxR;
-constexpr int kMaxStripes = TPZ_SW_MAX_QLEN / kStripeRows;
+constexpr int kMaxStripes = (TPZ_SW_MAX_QLEN + kStripeRows - 1) / kStripeRows;
 // row bins: b < 32 -> R = b+1, one stripe; b = 32..38 -> R = 32, b-30 stripes
 constexpr int kRBins = 40;
 constexpr int kSBins = 256;         // subject-length buckets (32 residues each)
@@ -223,7 +231,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
 
     uint32_t outH = 0u, outF = 0u, outFm = 0u;
     uint32_t diag = 0u;
-    uint32_t runmax = 0u;
+    uint32_t runmax = 0u, wmax = 0u;
     int colA = -1, rowA = 0, colB = -1, rowB = 0;
 
     // profile words of this step's column (j = k - lane), fetched one step
@@ -239,12 +247,19 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     }
     uint32_t let1 = ring[(1 - lane) & (kRing - 1)];
 
-    const int steps = N + 31;
-    for (int k = 0; k < steps; ++k) {
+    auto step = [&](const int k, const uint32_t (&cwa)[W], const uint32_t (&cwb)[W],
+                    uint32_t (&nwa)[W], uint32_t (&nwb)[W]) {
         const int j = k - lane;
         if ((k & 31) == 0 && k > 0) {
             ring[(k + 32 + lane) & (kRing - 1)] = (uint16_t)pre;
             pre = letter_pair(a, sA, slA, sB, slB, k + 64 + lane);
+            // warp maximum so far: a lane's rise below it cannot end up as
+            // the alignment's maximum, so it needs no row search
+            uint32_t wm = runmax;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                wm = __vimax_s16x2_relu(wm, __shfl_xor_sync(0xFFFFFFFFu, wm, o));
+            wmax = wm;
             __syncwarp();
         }
         uint32_t inH = __shfl_up_sync(0xFFFFFFFFu, outH, 1);
@@ -259,18 +274,19 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             }
         }
         // next step's profile words
-        uint32_t na[W], nb[W];
 #pragma unroll
         for (int w = 0; w < W; ++w) {
-            na[w] = profA[((let1 & 0xFFu) * W + w) * 32 + lane];
-            nb[w] = profB[((let1 >> 8) * W + w) * 32 + lane];
+            nwa[w] = profA[((let1 & 0xFFu) * W + w) * 32 + lane];
+            nwb[w] = profB[((let1 >> 8) * W + w) * 32 + lane];
         }
         let1 = ring[(j + 2) & (kRing - 1)];
+        bool need = false;
+        uint32_t cmx = 0u, thr = 0u;
         if (j >= 0 && j < N) {
             uint32_t F = inF, Fm = inFm, D = diag;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const uint32_t sc = prmt(wa[r >> 2], wb[r >> 2], SEL[r & 3]);
+                const uint32_t sc = prmt(cwa[r >> 2], cwb[r >> 2], SEL[r & 3]);
                 const uint32_t X = __viaddmax_s16x2_relu(D, sc, E[r]);
                 const uint32_t Hn = __vimax_s16x2_relu(X, F);
                 const uint32_t Xg = __viaddmax_s16x2(X, NGO, NEGINF);
@@ -281,11 +297,18 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
                 D = H[r];
                 H[r] = Hn;
             }
-            // column maximum of the lane's rows (all H >= 0)
-            uint32_t cm = H[0];
+            // column maximum of the lane's rows, floored at the search
+            // threshold max(running max, warp maximum - 1): a half needs its
+            // row found when it rises above the threshold, i.e. above the
+            // lane's running max and not below the warp maximum of the last
+            // refresh (anything lower cannot be the alignment maximum).  The
+            // running max may so take the value warp maximum - 1 without a
+            // cell holding it; such a lane can never hold the final maximum.
+            thr = __viaddmax_s16x2(wmax, 0xFFFFFFFFu, runmax);
+            uint32_t cm = thr;
 #pragma unroll
-            for (int r = 1; r + 1 < R; r += 2) cm = __vimax3_s16x2(cm, H[r], H[r + 1]);
-            if ((R & 1) == 0) cm = __vimax_s16x2_relu(cm, H[R - 1]);
+            for (int r = 0; r + 1 < R; r += 2) cm = __vimax3_s16x2(cm, H[r], H[r + 1]);
+            if (R & 1) cm = __vimax_s16x2_relu(cm, H[R - 1]);
             outH = H[R - 1];
             outF = F;
             outFm = Fm;
@@ -293,30 +316,41 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
                 uint32_t *b = bnd + 3 * (size_t)j;
                 b[0] = outH; b[1] = outF; b[2] = outFm;
             }
-            const uint32_t nm = __vimax_s16x2_relu(runmax, cm);
-            if (nm != runmax) {
-                // the lane's running max rose in this column: remember the
-                // column and the smallest row holding the new value
-                if (lo16(nm) != lo16(runmax)) {
-                    const int v = lo16(nm);
-                    int rr = R;
+            need = cm != thr;
+            runmax = cm;
+            cmx = cm;
+        }
+        if (__any_sync(0xFFFFFFFFu, need)) {
+            // smallest row holding the column maximum, both halves at once:
+            // max(H - cm, -1) is 0 on rows holding it and -1 elsewhere; those
+            // rows contribute R - r and the largest contribution wins
+            const uint32_t negv = __viaddmax_s16x2(~cmx, 0x00010001u, NEGINF);
+            uint32_t acc = 0u;
 #pragma unroll
-                    for (int r = R - 1; r >= 0; --r) if (lo16(H[r]) == v) rr = r;
-                    colA = j; rowA = i0 + rr;
+            for (int r = 0; r < R; r += 2) {
+                const uint32_t g0 =
+                    ~__viaddmax_s16x2(H[r], negv, 0xFFFFFFFFu) & pack2(R - r, R - r);
+                if (r + 1 < R) {
+                    const uint32_t g1 = ~__viaddmax_s16x2(H[r + 1], negv, 0xFFFFFFFFu) &
+                                        pack2(R - r - 1, R - r - 1);
+                    acc = __vimax3_s16x2(acc, g0, g1);
+                } else {
+                    acc = __vimax_s16x2_relu(acc, g0);
                 }
-                if (hi16(nm) != hi16(runmax)) {
-                    const int v = hi16(nm);
-                    int rr = R;
-#pragma unroll
-                    for (int r = R - 1; r >= 0; --r) if (hi16(H[r]) == v) rr = r;
-                    colB = j; rowB = i0 + rr;
-                }
-                runmax = nm;
+            }
+            if (need) {
+                if (lo16(cmx) > lo16(thr)) { colA = j; rowA = i0 + R - lo16(acc); }
+                if (hi16(cmx) > hi16(thr)) { colB = j; rowB = i0 + R - hi16(acc); }
             }
         }
         diag = inH;
-#pragma unroll
-        for (int w = 0; w < W; ++w) { wa[w] = na[w]; wb[w] = nb[w]; }
+    };
+    uint32_t wa2[W], wb2[W];
+    // an even step count; a step past N + 30 finds every lane past the end
+    const int steps = (N + 32) & ~1;
+    for (int k = 0; k < steps; k += 2) {
+        step(k, wa, wb, wa2, wb2);
+        step(k + 1, wa2, wb2, wa, wb);
     }
 
     kA = max(kA, best_key(lo16(runmax), colA, rowA));
