@@ -236,6 +236,43 @@ def search_bench(args, dev):
     return out
 
 
+def per_pair_bench(torch, t, ps, mat, dev, batched_gcups, npairs=20000, nstreams=(1, 16)):
+    """GCUPS of one kernel launch per pair (tpz_sw_align_one) on an evenly
+    spaced sample of the workload's pairs with qlen <= 1024, launched from
+    one host thread round-robin over 1 and over 16 CUDA streams."""
+    from topaz_b200 import native
+    idx = np.linspace(0, ps.n - 1, npairs).astype(np.int64)
+    idx = idx[ps.qlen[idx] <= 1024]
+    cells = int((ps.qlen[idx].astype(np.int64) * ps.slen[idx]).sum())
+    out = torch.empty((len(idx), 4), dtype=torch.int32, device=dev)
+    matc = np.ascontiguousarray(mat, dtype=np.int8)
+    L = native.lib()
+    qb, sb, ob = t["q"].data_ptr(), t["s"].data_ptr(), out.data_ptr()
+    qoff, qlen, soff, slen = ps.qoff[idx], ps.qlen[idx], ps.soff[idx], ps.slen[idx]
+    res = {"pairs": len(idx), "cells": cells, "api": "tpz_sw_align_one"}
+    for ns in nstreams:
+        streams = [torch.cuda.Stream(device=dev) for _ in range(ns)]
+        handles = [st.cuda_stream for st in streams]
+        for i in range(min(64, len(idx))):            # warm-up
+            native.check(L.tpz_sw_align_one(qb + int(qoff[i]), int(qlen[i]), sb + int(soff[i]),
+                                            int(slen[i]), matc.ctypes.data, 11, 1, ob + 16 * i,
+                                            handles[i % ns]))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(len(idx)):
+            native.check(L.tpz_sw_align_one(qb + int(qoff[i]), int(qlen[i]), sb + int(soff[i]),
+                                            int(slen[i]), matc.ctypes.data, 11, 1, ob + 16 * i,
+                                            handles[i % ns]))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        got = out.cpu().numpy()
+        ok = bool((got[:, 0] == t["score"][torch.from_numpy(idx).to(dev)].cpu().numpy()).all())
+        res["streams_%d" % ns] = {"gcups": round(cells / dt / 1e9, 3), "seconds": round(dt, 3),
+                                  "scores_match_batched": ok,
+                                  "batched_over_per_pair": round(batched_gcups / (cells / dt / 1e9), 1)}
+    return res
+
+
 def native_arm(args, rank, local_rank, world):
     import torch
     import torch.distributed as dist
@@ -339,6 +376,12 @@ def native_arm(args, rank, local_rank, world):
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in outs.values())
 
+    # the plain per-pair-launch GPU form: one tpz_sw_align_one launch per pair
+    # (the per-hit ssw_init + ssw_align pattern moved to the GPU) on a sample
+    per_pair = None
+    if rank == 0:
+        per_pair = per_pair_bench(torch, t, ps, mat, dev, achieved)
+
     line = None
     search = None
     if rank == 0 and world == 1 and not args.no_search:
@@ -367,6 +410,7 @@ def native_arm(args, rank, local_rank, world):
                                         % (dpx_ops_s, DPX_OPS_PER_CELL),
                          "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None)},
             "cpu_baseline": cpu,
+            "per_pair_gpu": per_pair,
             "clocks": clk,
             "step_ms": [round(x, 3) for x in step_ms],
             "search": search,

@@ -91,6 +91,16 @@ TPZ_API int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, c
                       const int8_t *mat625, int gap_open, int gap_extend,
                       int32_t *score, int32_t *ref_end, int32_t *read_end, int32_t *status);
 
+/* One pair, one kernel launch: the per-pair form of ssw_init + ssw_align
+ * (src/ssw_wrapper.c:157-245 calls them once per hit), with the same results
+ * as tpz_sw_batch_device.  q, s and out4 are device pointers (q and s in
+ * matrix-index residues, out4 = {score, ref_end, read_end, status}); the
+ * launch goes on `stream` and the call does not wait for it.  Limits:
+ * 1 <= qlen <= 1024, and qlen * (largest matrix entry) < 32512. */
+TPZ_API int tpz_sw_align_one(const int8_t *q, int32_t qlen, const int8_t *s, int32_t slen,
+                             const int8_t *mat625_host, int gap_open, int gap_extend,
+                             int32_t *out4, void *stream);
+
 /* Allocation-free variant of tpz_sw_batch_device, with no counterpart in the
  * TOPAZ reference.  For callers that must not have device memory allocated
  * on their behalf -- e.g. a server whose HBM is planned around a resident

@@ -136,3 +136,36 @@ def test_sw_long_queries_multi_stripe(cuda):
     assert (ref[0] == 32747).any() and (ref[3] == native.TPZ_SW_DROPPED).any()
     host = np.stack(native.sw_batch_host(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat))
     assert (host == ref).all()
+
+
+def test_sw_align_one_matches_reference_golden(cuda, golden_sw):
+    """The per-pair launch form (tpz_sw_align_one) gives the reference's
+    ssw_align results pair by pair, saturating u8 passes included."""
+    torch = cuda
+    g = golden_sw
+    d = torch.device("cuda:0")
+    q = torch.from_numpy(np.ascontiguousarray(g["q"])).to(d)
+    s = torch.from_numpy(np.ascontiguousarray(g["s"])).to(d)
+    n = len(g["qlen"])
+    for key, mat, go, ge in _settings(g):
+        out = torch.full((n, 4), -7, dtype=torch.int32, device=d)
+        st = torch.cuda.current_stream().cuda_stream
+        for i in range(n):
+            native.sw_align_one(q.data_ptr() + int(g["qoff"][i]), g["qlen"][i],
+                                s.data_ptr() + int(g["soff"][i]), g["slen"][i], mat, go, ge,
+                                out.data_ptr() + 16 * i, st)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().T
+        bad = np.flatnonzero((got != g[key]).any(axis=0))
+        assert bad.size == 0, (key, bad[:5], got[:, bad[:5]], g[key][:, bad[:5]])
+
+
+def test_sw_align_one_rejects_out_of_range(cuda):
+    torch = cuda
+    out = torch.zeros(4, dtype=torch.int32, device="cuda:0")
+    q = torch.zeros(2048, dtype=torch.int8, device="cuda:0")
+    mat = synth.matrix("BLOSUM62")
+    with pytest.raises(native.TopazError):
+        native.sw_align_one(q.data_ptr(), 1025, q.data_ptr(), 10, mat, 11, 1, out.data_ptr())
+    with pytest.raises(native.TopazError):
+        native.sw_align_one(q.data_ptr(), 10, q.data_ptr(), 10, mat, 1, 1, out.data_ptr())

@@ -426,6 +426,39 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
     }
 }
 
+// One pair per launch (the per-pair form of ssw_init + ssw_align): the u8
+// lane pass and, when it saturates, the i16 lane pass in the same launch.
+// Pair lengths and the rerun flag live in shared memory.
+template <int R>
+__global__ void __launch_bounds__(32) sw_one_kernel(const __grid_constant__ Args a, int qlen,
+                                                    int slen) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ int64_t s_off;
+    __shared__ int32_t s_ql, s_sl, s_rr[2];
+    int8_t *smat = reinterpret_cast<int8_t *>(smem);
+    uint32_t *profA = reinterpret_cast<uint32_t *>(smem + kSmatBytes);
+    uint32_t *profB = profA + profile_bytes(R) / 4;
+    uint16_t *ring = reinterpret_cast<uint16_t *>(profB + profile_bytes(R) / 4);
+    const int lane = threadIdx.x;
+    for (int i = lane; i < 26 * kMatStride; i += 32) {
+        const int r = i / kMatStride, c = i % kMatStride;
+        smat[i] = (r < 25 && c < 25) ? a.mat[r * 25 + c] : (int8_t)kPadScore;
+    }
+    if (lane == 0) { s_off = 0; s_ql = qlen; s_sl = slen; s_rr[0] = 0; s_rr[1] = 0; }
+    __syncwarp();
+    Args b = a;
+    b.qoff = &s_off; b.soff = &s_off; b.qlen = &s_ql; b.slen = &s_sl;
+    b.rerun_count = &s_rr[0]; b.rerun = &s_rr[1];
+    b.ssw_lanes = 16;
+    run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr);
+    __syncwarp();
+    if (s_rr[0]) {
+        // the u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
+        b.ssw_lanes = 8;
+        run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr);
+    }
+}
+
 // ---------------------------------------------------------------- binning
 
 __device__ __forceinline__ int pair_bin(int ql, int sl) {
@@ -818,6 +851,52 @@ int ensure(size_t bytes) {
 
 }  // namespace
 
+namespace tpz {
+namespace sw {
+
+constexpr int kOneMaxQlen = kStripeRows;
+
+typedef void (*OneFn)(const Args, int, int);
+
+template <int R>
+struct OneTable {
+    static void fill(OneFn *k) {
+        k[R - 1] = sw_one_kernel<R>;
+        OneTable<R - 1>::fill(k);
+    }
+};
+template <>
+struct OneTable<0> {
+    static void fill(OneFn *) {}
+};
+
+struct OneCfg {
+    OneFn fn[kMaxR];
+};
+
+static int one_cfg(const OneCfg **out) {
+    static std::mutex mu;
+    static std::vector<OneCfg *> per_dev;
+    int dev = 0;
+    TPZ_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, nullptr);
+    if (!per_dev[dev]) {
+        OneCfg *c = new OneCfg();
+        OneTable<kMaxR>::fill(c->fn);
+        for (int r = 1; r <= kMaxR; ++r)
+            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          smem_bytes(r)));
+        per_dev[dev] = c;
+    }
+    *out = per_dev[dev];
+    return TPZ_OK;
+}
+
+}  // namespace sw
+}  // namespace tpz
+
 extern "C" {
 
 int tpz_sw_batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
@@ -889,6 +968,41 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
 }
 
 int64_t tpz_sw_last_launches(void) { return tpz::sw::g_last_launches; }
+
+int tpz_sw_align_one(const int8_t *q, int32_t qlen, const int8_t *s, int32_t slen,
+                     const int8_t *mat625_host, int gap_open, int gap_extend, int32_t *out4,
+                     void *stream) {
+    using namespace tpz::sw;
+    if (!q || !s || !out4 || !mat625_host || qlen < 1 || qlen > kOneMaxQlen || slen < 0 ||
+        slen >= TPZ_SW_MAX_SLEN) {
+        tpz::set_error("tpz_sw_align_one: need 1 <= qlen <= 1024, 0 <= slen < 2^24, non-NULL buffers");
+        return TPZ_E_ARG;
+    }
+    if (!(gap_open > gap_extend && gap_extend >= 0 && gap_open <= 255)) {
+        tpz::set_error("tpz_sw_align_one: requires 255 >= gap_open > gap_extend >= 0");
+        return TPZ_E_ARG;
+    }
+    const OneCfg *cfg = nullptr;
+    int rc = one_cfg(&cfg);
+    if (rc) return rc;
+    int mn = 0, mx = 0;
+    for (int i = 0; i < 625; ++i) { mn = std::min<int>(mn, mat625_host[i]); mx = std::max<int>(mx, mat625_host[i]); }
+    if ((int64_t)qlen * mx >= kBig) {
+        tpz::set_error("tpz_sw_align_one: matrix entries too large for 16-bit scores at this length");
+        return TPZ_E_ARG;
+    }
+    Args a;
+    memset(&a, 0, sizeof a);
+    a.q = q; a.s = s;
+    a.score = out4; a.ref_end = out4 + 1; a.read_end = out4 + 2; a.status = out4 + 3;
+    a.gap_open = gap_open; a.gap_extend = gap_extend; a.bias = -mn;
+    memcpy(a.mat, mat625_host, 625);
+    a.exact_threshold = 32767;
+    const int R = (qlen + 31) / 32;
+    cfg->fn[R - 1]<<<1, 32, smem_bytes(R), (cudaStream_t)stream>>>(a, qlen, slen);
+    TPZ_CUDA(cudaGetLastError());
+    return TPZ_OK;
+}
 
 int tpz_dpx_probe(int64_t blocks, int iters, uint32_t *out, void *stream, int64_t *ops) {
     if (blocks < 1 || iters < 1 || !out || !ops) { tpz::set_error("tpz_dpx_probe: bad argument"); return TPZ_E_ARG; }

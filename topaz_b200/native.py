@@ -50,6 +50,7 @@ def lib():
     L.tpz_sw_batch_host.argtypes = sw_args
     L.tpz_sw_batch_device.argtypes = sw_args + [_VP]
     L.tpz_sw_last_launches.restype = ctypes.c_int64
+    L.tpz_sw_align_one.argtypes = [_VP, _I32, _VP, _I32, _VP, _I32, _I32, _VP, _VP]
     L.tpz_dpx_probe.argtypes = [_I64, _I32, _VP, _VP, _VP]
     _LIB = L
     return L
@@ -106,6 +107,15 @@ def sw_batch_torch(t, mat, gap_open=11, gap_extend=1, stream=None):
                     t["slen"].data_ptr(), mat, gap_open, gap_extend, t["score"].data_ptr(),
                     t["ref_end"].data_ptr(), t["read_end"].data_ptr(), t["status"].data_ptr(),
                     st.cuda_stream)
+
+
+def sw_align_one(q_ptr, qlen, s_ptr, slen, mat, gap_open, gap_extend, out4_ptr, stream=0):
+    """One pair, one kernel launch (tpz_sw_align_one): device pointers to the
+    query and subject (matrix indices) and to 4 int32 outputs {score,
+    ref_end, read_end, status}; enqueued on `stream` (a cudaStream_t)."""
+    L = lib()
+    check(L.tpz_sw_align_one(q_ptr, int(qlen), s_ptr, int(slen), _p(np.ascontiguousarray(mat, np.int8)),
+                             gap_open, gap_extend, out4_ptr, stream))
 
 
 def last_launches() -> int:
