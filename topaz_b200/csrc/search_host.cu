@@ -643,7 +643,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         (rc = b.alloc(&dsub, 625)) || (rc = b.alloc(&dcur, 2 * npos + 1)) ||
         (rc = b.alloc(&dscratch, per_q * nq)) || (rc = b.alloc(&dhits, (size_t)nq * max_cap)) ||
         (rc = b.alloc(&dqout, nq)) || (rc = b.alloc(&dqnext, 2 * npos + 1)) ||
-        (rc = b.alloc(&dcache, 32 * (2 * npos + 1))))
+        (rc = b.alloc(&dcache, (size_t)kChain * (2 * npos + 1))))
         return rc;
     if (o->trace_pops > 0 && (rc = b.alloc(&dtrace, (size_t)nq * o->trace_pops))) return rc;
     TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
@@ -665,7 +665,10 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         SeedArgs sa;
         sa.qcat = dq; sa.qoff = dqo; sa.qlen = dql; sa.pos_base = dpb; sa.nq = (int)nq;
         sa.npos = npos; sa.sub = dsub; sa.cursors = dcur; sa.lb_out = nullptr; sa.qstatus = dqs;
+        sa.chain = kChain;
         seed_kernel<<<(unsigned)std::min<int64_t>((npos + 127) / 128, (int64_t)nsm * 16), 128>>>(ix->d, sa);
+        chain_kernel<<<(unsigned)std::min<int64_t>((2 * npos * kChain + 255) / 256, (int64_t)nsm * 64),
+                       256>>>(ix->d, sa, o->min_hit_length, dcache);
     }
     WalkArgs wa;
     wa.qcat = dq; wa.qoff = dqo; wa.qlen = dql; wa.nq = (int)nq; wa.cursor_base = dcb;

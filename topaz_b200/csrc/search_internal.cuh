@@ -28,6 +28,7 @@ struct Cursor {
 };
 
 constexpr int kWalkWarps = 4;            // queries (warps) per walk block
+constexpr int kChain = 32;               // chain elements cached per cursor
 
 struct Hit {
     int32_t protein, gapless_score, gapless_length, suffix_offset;
@@ -54,6 +55,7 @@ struct SeedArgs {
     Cursor *cursors;           // 2 per position
     int64_t *lb_out;           // optional: bound per position (-2 skipped)
     int32_t *qstatus;          // per query status bits
+    int chain;                 // chain elements precomputed per cursor (0 or kChain)
 };
 
 struct WalkArgs {
@@ -81,6 +83,7 @@ __global__ void nl_block_count_kernel(const uint8_t *T, int64_t Tsize, int64_t n
 __global__ void lb_build_kernel(const uint8_t *T, int64_t Tsize, const int64_t *SA, int64_t *lb);
 __global__ void seed_kernel(DevIndex ix, SeedArgs a);
 __global__ void walk_kernel(DevIndex ix, WalkArgs a);
+__global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32_t *cache);
 __global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t *qoff,
                                  const int32_t *qlen, const int32_t *query_of, const int32_t *off,
                                  const int64_t *row, int64_t n, const int8_t *sub, int32_t *score,

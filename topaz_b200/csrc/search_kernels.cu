@@ -200,8 +200,8 @@ __global__ void seed_kernel(DevIndex ix, SeedArgs a) {
         const uint8_t *Q = a.qcat + a.qoff[q];
         const int qlen = a.qlen[q];
         Cursor c0, c1;
-        c0.row = -1; c0.off = i; c0.dir = 1; c0.cpos = 0; c0.cn = 0; c0.score = 0; c0.len = -1;
-        c1.row = -1; c1.off = i; c1.dir = -1; c1.cpos = 0; c1.cn = 0; c1.score = 0; c1.len = -1;
+        c0.row = -1; c0.off = i; c0.dir = 1; c0.cpos = 0; c0.cn = a.chain; c0.score = 0; c0.len = -1;
+        c1.row = -1; c1.off = i; c1.dir = -1; c1.cpos = 0; c1.cn = a.chain; c1.score = 0; c1.len = -1;
         if (Q[i] != 'V') {                     // _bad_prefix: internal 'V' = X
             const int64_t pos = lower_bound(ix, Q + i, qlen - i);
             if (a.lb_out) a.lb_out[g] = pos;
@@ -287,6 +287,41 @@ __device__ __forceinline__ uint32_t pack_elem(int score, int len) {
 }
 __device__ __forceinline__ int elem_score(uint32_t e) { return (int)(int16_t)(e & 0xFFFFu); }
 __device__ __forceinline__ int elem_len(uint32_t e) { return (int)(int16_t)(e >> 16); }
+
+// The chain element of a cursor `step` rows past `row` (step >= 1): the
+// sa_hsp (src/suffix.c:47) of suffix_increment's next row, or a marker.
+__device__ __forceinline__ uint32_t chain_elem(const DevIndex &ix, int64_t row, int dir, int step,
+                                               const uint8_t *Q, int qlen, int off,
+                                               const int8_t *sub) {
+    const int64_t nr = row + (int64_t)dir * step;
+    if (nr < 0 || nr >= 8 * ix.Tsize) return pack_elem(0, kLenEnd);
+    if (nr >= ix.sa_rows) return pack_elem(0, kLenFault);
+    int sc = 0;
+    const int ln = hsp_at(ix, ix.SA[nr], Q, qlen, off, sub, &sc);
+    return pack_elem(sc, ln);
+}
+
+// One thread per (cursor, element): the first kChain chain elements of every
+// queued cursor, so that the walk, whose pops run one after another, finds
+// them ready.  Elements a cursor never reaches are computed and not used.
+__global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32_t *cache) {
+    const int64_t total = 2 * a.npos * kChain;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total;
+         x += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = x / kChain;
+        const int e = (int)(x % kChain);
+        const Cursor cu = a.cursors[c];
+        if (cu.len < min_hit_length) continue;          // never queued
+        const int64_t g = c >> 1;
+        int lo = 0, hi = a.nq - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.pos_base[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        cache[x] = chain_elem(ix, cu.row, cu.dir, e + 1, a.qcat + a.qoff[lo], a.qlen[lo], cu.off,
+                              a.sub);
+    }
+}
 
 struct HitView {
     int32_t *hprot, *hscore, *hlen, *hoff, *hprev, *hnext, *hfree;   // cap+1 slots
@@ -405,16 +440,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
             row = __shfl_sync(0xFFFFFFFFu, row, 0);
             off = __shfl_sync(0xFFFFFFFFu, off, 0);
             dir = __shfl_sync(0xFFFFFFFFu, dir, 0);
-            const int64_t nr = row + (int64_t)dir * (lane + 1);
-            if (nr < 0 || nr >= 8 * ix.Tsize) {
-                elem = pack_elem(0, kLenEnd);
-            } else if (nr >= ix.sa_rows) {
-                elem = pack_elem(0, kLenFault);
-            } else {
-                int sc = 0;
-                const int ln = hsp_at(ix, ix.SA[nr], Q, qlen, off, a.sub, &sc);
-                elem = pack_elem(sc, ln);
-            }
+            elem = chain_elem(ix, row, dir, lane + 1, Q, qlen, off, a.sub);
             cache[(int64_t)c * 32 + lane] = elem;
             __syncwarp();
         }
