@@ -47,7 +47,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--search-batch", type=int, default=5000,
+    ap.add_argument("--search-workers", type=int, default=2,
+                    help="host threads issuing search batches concurrently")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop section")
+    ap.add_argument("--search-batch", type=int, default=2500,
                     help="queries per tpz_search_batch call in the full-search section")
     ap.add_argument("--no-search", action="store_true",
                     help="skip the full-search (config 2) section")
@@ -82,6 +85,11 @@ class ClockSampler:
             return
         self.th = threading.Thread(target=self._read, daemon=True)
         self.th.start()
+        # nvidia-smi's start-up holds the driver for a moment: wait for its
+        # first sample so that it falls outside the timed region
+        t0 = time.perf_counter()
+        while not self.rows and time.perf_counter() - t0 < 10 and self.proc.poll() is None:
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -151,6 +159,54 @@ SEARCH_WORKLOAD = ("full search, mid size: 1,000,000-protein synthetic DB (log-n
                    "batches of %d queries")
 
 
+SERVE_WORKLOAD = ("serving on the resident mid-size DB: Poisson request arrivals at 5 offered "
+                  "loads (fractions of the measured batch throughput), each request 1-1000 "
+                  "queries (log-uniform count) of 30-3000 residues, continuous batching across "
+                  "requests by %d worker threads (batches up to %d queries, admitted by free "
+                  "device memory), -H 100 -E 1e-3")
+
+
+def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.8, 1.0),
+                seconds=6.0):
+    """p50/p99 request latency and delivered queries/s of the serving loop
+    (topaz_b200.serve.SearchServer) at five offered loads."""
+    from topaz_b200 import native, serve, synth
+    qres, qlens = synth.search_queries_arrays(res, lens, 4000, 4000, seed=args.seed + 21,
+                                              lo=30, hi=3000)
+    qoff = np.cumsum(qlens) - qlens
+    pool = [native.prepare_query(qres[o:o + n].tobytes()) for o, n in zip(qoff, qlens)]
+    rng = np.random.Generator(np.random.PCG64(args.seed + 22))
+    workers, max_batch = 3, 2000
+    srv = serve.SearchServer(ix, mat, workers=workers, max_batch=max_batch,
+                             report={"max_evalue": 1e-3})
+    srv.submit(pool[:50]).result()                        # warm-up
+    rows = []
+    mean_req = float(np.mean(np.exp(rng.uniform(0, np.log(1000), 100000))))
+    for load in loads:
+        qps = load * capacity_qps
+        rate = qps / mean_req                              # requests per second
+        futs, nq, t = [], 0, 0.0
+        t0 = time.perf_counter()
+        while t < seconds:
+            t += rng.exponential(1.0 / rate)
+            n = int(np.exp(rng.uniform(0, np.log(1000))))
+            start = int(rng.integers(0, len(pool) - n))
+            while time.perf_counter() - t0 < t:
+                time.sleep(0.0005)
+            futs.append(srv.submit(pool[start:start + n]))
+            nq += n
+        for f in futs:
+            f.result()
+        wall = time.perf_counter() - t0
+        lat = np.array([serve.latency_of(f) for f in futs]) * 1e3
+        rows.append({"offered_qps": round(qps, 1), "requests": len(futs), "queries": nq,
+                     "delivered_qps": round(nq / wall, 1), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                     "p99_ms": round(float(np.percentile(lat, 99)), 2)})
+    srv.close()
+    return {"workload": SERVE_WORKLOAD % (workers, max_batch), "capacity_qps": round(capacity_qps, 1),
+            "loads": rows, "api": "topaz_b200.serve.SearchServer over tpz_search_batch report mode"}
+
+
 def search_bench(args, dev):
     """Full-search throughput (queries/s) through tpz_search_batch with host
     buffers (SEG + internal alphabet on the host, H2D of queries, D2H of
@@ -182,23 +238,45 @@ def search_bench(args, dev):
     torch.cuda.synchronize()
     bsz = args.search_batch
     stage = np.zeros(4)
-    nh = 0
+    nh = [0]
+    starts = list(range(0, len(q_aa), bsz))
+    lock = threading.Lock()
+
+    def worker():
+        # batches taken in order by host threads, each thread on its own CUDA
+        # default stream, so one batch's SW overlaps another's walk
+        while True:
+            with lock:
+                if not starts:
+                    return
+                b = starts.pop(0)
+            qs = [native.prepare_query(q) for q in q_aa[b:b + bsz]]
+            r = ix.search(qs, mat, report=report)
+            with lock:
+                stage[:] += np.array(r["stage_ms"])
+                nh[0] += len(r["protein"])
+
     t0 = time.perf_counter()
-    for b in range(0, len(q_aa), bsz):
-        qs = [native.prepare_query(q) for q in q_aa[b:b + bsz]]
-        r = ix.search(qs, mat, report=report)
-        stage += np.array(r["stage_ms"])
-        nh += len(r["protein"])
+    th = [threading.Thread(target=worker) for _ in range(args.search_workers)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
     wall = time.perf_counter() - t0
+    nh = nh[0]
     out = {"workload": SEARCH_WORKLOAD % bsz, "queries": len(q_aa), "queries_per_s": round(len(q_aa) / wall, 1),
            "wall_s": round(wall, 3),
            "api": "tpz_search_batch report mode (host buffers; SEG + alphabet on the host, "
-                  "ranking and -H/-E cut on the device, all inside the timed region)",
+                  "ranking and -H/-E cut on the device, all inside the timed region; "
+                  "batches from %d host threads)" % args.search_workers,
            "device_ms": {"seed": round(stage[0], 2), "walk_hitlist": round(stage[1], 2),
                          "sw_rank_select": round(stage[2], 2), "calls_wall": round(stage[3], 2)},
            "reported_hits_per_query": round(nh / len(q_aa), 2),
+           "host_threads": args.search_workers,
            "setup_s": round(setup_s, 1), "index_load_s": round(load_s, 2),
            "index_device_gb": round(ix.device_bytes / 1e9, 2)}
+    if not args.no_serve:
+        out["serving"] = serve_bench(ix, mat, res, lens, len(q_aa) / wall, args)
     ix.close()
     if args.no_cpu_baseline or not os.path.exists(oracle.REF_BIN):
         return out

@@ -177,3 +177,28 @@ def test_index_rejects_inconsistent_files(cuda, fresh):
     sa[10] = db.Tsize + 5
     with pytest.raises(native.TopazError):
         native.Index(dbformat.Database(db.T, sa, db.ind, db.headers))
+
+
+def test_search_concurrent_calls_match_sequential(cuda, fresh):
+    """tpz_search_batch from several host threads at once (each thread on its
+    own default stream) gives each caller what it gets alone."""
+    import threading
+    db, qs = fresh
+    ix = native.Index(db)
+    parts = [qs[i::3] for i in range(3)]
+    rep = {"max_evalue": 10.0}
+    alone = [ix.search(p, BLOSUM62, report=rep) for p in parts]
+    got = [None] * len(parts)
+
+    def run(i):
+        for _ in range(2):
+            got[i] = ix.search(parts[i], BLOSUM62, report=rep)
+
+    th = [threading.Thread(target=run, args=(i,)) for i in range(len(parts))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for a, b in zip(alone, got):
+        for k in ("hit_off", "protein", "rawscore", "qend", "send", "bitscore", "evalue", "npops"):
+            assert np.array_equal(a[k], b[k]), k

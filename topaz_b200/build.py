@@ -55,6 +55,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         obj = os.path.join(LIBDIR, os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
+               "--default-stream", "per-thread",
                "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

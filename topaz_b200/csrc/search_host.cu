@@ -55,13 +55,30 @@ int dalloc(tpz_index *ix, void **p, size_t bytes) {
     return TPZ_OK;
 }
 
+// Per-call device buffers, stream-ordered on the calling thread's default
+// stream (the library is built with per-thread default streams), so calls
+// from different host threads neither wait for each other's allocations nor
+// for each other's kernels.  The pool keeps freed memory for the next call.
+void keep_pool_memory() {
+    static thread_local int done_dev = -1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev == done_dev) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done_dev = dev;
+}
+
 struct DevBuf {
     std::vector<void *> ptrs;
-    ~DevBuf() { for (void *p : ptrs) cudaFree(p); }
+    DevBuf() { keep_pool_memory(); }
+    ~DevBuf() { for (void *p : ptrs) cudaFreeAsync(p, cudaStreamPerThread); }
     template <class T>
     int alloc(T **p, size_t count) {
         void *q = nullptr;
-        TPZ_CUDA(cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)));
+        TPZ_CUDA(cudaMallocAsync(&q, std::max<size_t>(count * sizeof(T), 16), cudaStreamPerThread));
         ptrs.push_back(q);
         *p = (T *)q;
         return TPZ_OK;
@@ -786,7 +803,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         r.bitscore = R->bits.data();
         r.evalue = R->evalue.data();
     }
-    TPZ_CUDA(cudaDeviceSynchronize());
+    TPZ_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
     float t01 = 0, t12 = 0, t23 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
     cudaEventElapsedTime(&t12, ev[1], ev[2]);

@@ -580,12 +580,28 @@ struct LaunchCfg {
     cudaEvent_t fork, join[kAuxStreams];
 };
 
+// Per host thread and device: the auxiliary streams and fork/join events of
+// one call must not be shared with a call running in another thread.
+struct LaunchCfgs {
+    std::vector<LaunchCfg *> per_dev;
+    ~LaunchCfgs() {
+        for (LaunchCfg *c : per_dev) {
+            if (!c) continue;
+            for (int i = 0; i < kAuxStreams; ++i) {
+                cudaStreamDestroy(c->aux[i]);
+                cudaEventDestroy(c->join[i]);
+            }
+            cudaEventDestroy(c->fork);
+            delete c;
+        }
+    }
+};
+
 static int launch_cfg(const LaunchCfg **out) {
-    static std::mutex mu;
-    static std::vector<LaunchCfg *> per_dev;
+    static thread_local LaunchCfgs cfgs;
+    std::vector<LaunchCfg *> &per_dev = cfgs.per_dev;
     int dev = 0;
     TPZ_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
     if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, nullptr);
     if (!per_dev[dev]) {
         LaunchCfg *c = new LaunchCfg();

@@ -1,0 +1,177 @@
+"""Search serving: a continuous-batching request loop over a resident index.
+
+Requests (lists of queries, internal alphabet after SEG, as
+``native.prepare_query`` makes them) arrive through ``submit``.  Worker
+threads -- each one a host thread with its own CUDA default stream, so their
+batches run on the device at the same time -- take every waiting query, in
+arrival order and across request boundaries, up to ``max_batch`` queries and
+up to the device memory still free under ``mem_budget``, run them through
+``tpz_search_batch`` in report mode, and hand each query's reported hits back
+to its request.  A request completes when its last query is back; a request
+that arrives while others are on the GPU is admitted as soon as a worker and
+memory are free, so short requests are not held behind long ones.
+
+Each query's result does not depend on the queries batched with it (every
+query has its own walk, hitlist and SW pairs), so a request gets the same
+hits alone and in a mix; the tests check exactly that.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+
+from . import native
+
+
+def query_device_bytes(qlen: int, num_hits: int = 100, alignments: int = 5000,
+                       min_hit_length: int = 5) -> int:
+    """Upper estimate of the device memory one query takes inside
+    tpz_search_batch: cursors, chain caches and queue links per searched
+    position, the hitlist structures and the hit and SW arrays of its
+    hitlist capacity."""
+    cap = int(1.5 * num_hits) if qlen > 3000 else alignments
+    npos = max(0, qlen - min_hit_length)
+    hash_size = 16
+    while hash_size < 2 * (cap + 1):
+        hash_size <<= 1
+    per_pos = 2 * (24 + 4 + 4 * 32) + 8
+    hitlist = 7 * 4 * (cap + 1) + 2 * 4 * 4352 + 8 * 68 + 2 * 4 * hash_size
+    hits = cap * (16 + 4 * 24)
+    return npos * per_pos + hitlist + hits + qlen + 256
+
+
+class _Request:
+    __slots__ = ("queries", "results", "left", "future", "t_submit", "t_done")
+
+    def __init__(self, queries):
+        self.queries = queries
+        self.results = [None] * len(queries)
+        self.left = len(queries)
+        self.future = Future()
+        self.t_submit = time.perf_counter()
+        self.t_done = None
+
+
+class SearchServer:
+    """Continuous batching of search requests over one resident ``Index``."""
+
+    def __init__(self, index, mat, workers: int = 2, max_batch: int = 2000,
+                 mem_budget: int | None = None, report=None, search_kwargs=None):
+        self.ix = index
+        self.mat = np.ascontiguousarray(mat, dtype=np.int8)
+        self.max_batch = int(max_batch)
+        self.report = dict(report or {"max_evalue": 1e-3})
+        self.kw = dict(search_kwargs or {})
+        if mem_budget is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info()
+            mem_budget = int(0.8 * free)
+        self.mem_budget = int(mem_budget)
+        self._mem_used = 0
+        self._pending = collections.deque()     # (request, query index)
+        self._cv = threading.Condition()
+        self._closed = False
+        self.batches = []                       # (n queries, seconds) per finished batch
+        self._threads = [threading.Thread(target=self._work, daemon=True) for _ in range(workers)]
+        for t in self._threads:
+            t.start()
+
+    # -- client side
+    def submit(self, queries) -> Future:
+        """Queues a request; the future resolves to a list with, per query,
+        a dict of its reported hits (protein, rawscore, qend, send, bitscore,
+        evalue, sw_status, status)."""
+        req = _Request(list(queries))
+        req.future.request = req
+        if not req.queries:
+            req.t_done = req.t_submit
+            req.future.set_result([])
+            return req.future
+        with self._cv:
+            if self._closed:
+                raise RuntimeError("server is closed")
+            for i in range(len(req.queries)):
+                self._pending.append((req, i))
+            self._cv.notify_all()
+        return req.future
+
+    def close(self):
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        for t in self._threads:
+            t.join()
+
+    # -- worker side
+    def _take(self):
+        """The next batch: waiting queries in arrival order, as many as fit
+        max_batch and the free part of the memory budget (at least one)."""
+        with self._cv:
+            while True:
+                if self._pending:
+                    batch, need = [], 0
+                    while self._pending and len(batch) < self.max_batch:
+                        req, i = self._pending[0]
+                        b = query_device_bytes(len(req.queries[i]), **self._size_kw())
+                        if batch and self._mem_used + need + b > self.mem_budget:
+                            break
+                        if not batch and self._mem_used + b > self.mem_budget and self._mem_used:
+                            break                   # wait for memory to come back
+                        self._pending.popleft()
+                        batch.append((req, i))
+                        need += b
+                    if batch:
+                        self._mem_used += need
+                        return batch, need
+                if self._closed:
+                    return None, 0
+                self._cv.wait()
+
+    def _size_kw(self):
+        kw = {k: self.kw[k] for k in ("num_hits", "alignments", "min_hit_length") if k in self.kw}
+        return kw
+
+    def _work(self):
+        while True:
+            batch, need = self._take()
+            if batch is None:
+                return
+            t0 = time.perf_counter()
+            try:
+                r = self.ix.search([req.queries[i] for req, i in batch], self.mat,
+                                   report=self.report, **self.kw)
+                err = None
+            except Exception as e:              # hand the failure to every request
+                r, err = None, e
+            dt = time.perf_counter() - t0
+            done = []
+            with self._cv:
+                self._mem_used -= need
+                self.batches.append((len(batch), dt))
+                for k, (req, i) in enumerate(batch):
+                    if err is not None:
+                        if not req.future.done():
+                            req.t_done = time.perf_counter()
+                            req.future.set_exception(err)
+                        continue
+                    a, b = r["hit_off"][k], r["hit_off"][k + 1]
+                    req.results[i] = {f: r[f][a:b] for f in ("protein", "rawscore", "qend", "send",
+                                                              "bitscore", "evalue", "sw_status")}
+                    req.results[i]["status"] = int(r["status"][k])
+                    req.left -= 1
+                    if req.left == 0:
+                        req.t_done = time.perf_counter()
+                        done.append(req)
+                self._cv.notify_all()
+            for req in done:
+                req.future.set_result(req.results)
+
+
+def latency_of(future) -> float:
+    """Seconds from submit to completion of a finished request."""
+    req = future.request
+    return req.t_done - req.t_submit
