@@ -131,9 +131,11 @@ __global__ void pack_hits_kernel(PackArgs a) {
     }
 }
 
+// SW results of pair k back to hit p_hit[k]; hit2pair (optional) records k
 __global__ void scatter_sw_kernel(int64_t n, const int32_t *p_hit, const int32_t *sc,
                                   const int32_t *re, const int32_t *rd, const int32_t *st,
-                                  int32_t *raw, int32_t *send, int32_t *qend, int32_t *sw_status) {
+                                  int32_t *raw, int32_t *send, int32_t *qend, int32_t *sw_status,
+                                  int32_t *hit2pair) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int h = p_hit[k];
@@ -141,6 +143,34 @@ __global__ void scatter_sw_kernel(int64_t n, const int32_t *p_hit, const int32_t
         send[h] = re[k];
         qend[h] = rd[k];
         sw_status[h] = st[k];
+        if (hit2pair) hit2pair[h] = (int32_t)k;
+    }
+}
+
+// Pairs of the selected (reported) aligned hits, for the SW pass that finds
+// their end coordinates after a score-only pass over every hit.
+struct SelPairArgs {
+    const int32_t *sel, *nsel, *sw_status, *hit2pair;
+    int nq, top;
+    const int64_t *pq_off, *ps_off;
+    const int32_t *pq_len, *ps_len;
+    int64_t *lq_off, *ls_off;
+    int32_t *lq_len, *ls_len, *lhit, *count;
+};
+
+__global__ void selected_pairs_kernel(SelPairArgs a) {
+    const int64_t total = (int64_t)a.nq * a.top;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total;
+         x += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(x / a.top), t = (int)(x % a.top);
+        if (t >= a.nsel[q]) continue;
+        const int h = a.sel[x];
+        if (a.sw_status[h] != TPZ_SW_OK) continue;
+        const int k = a.hit2pair[h];
+        const int slot = atomicAdd(a.count, 1);
+        a.lq_off[slot] = a.pq_off[k]; a.lq_len[slot] = a.pq_len[k];
+        a.ls_off[slot] = a.ps_off[k]; a.ls_len[slot] = a.ps_len[k];
+        a.lhit[slot] = h;
     }
 }
 
@@ -351,10 +381,17 @@ bool letters_ok(const char *s, int64_t n) {
 
 // Report mode after the SW of a batch: rank, select and gather on the device,
 // then copy the reported hits and score them with tpz_karlin.
+struct HitPairs {                 // the SW pairs of a batch and where they came from
+    const int8_t *q, *T;
+    const int64_t *pq_off, *ps_off;
+    const int32_t *pq_len, *ps_len, *hit2pair;
+    const int8_t *xmap;           // host, 128 entries
+};
+
 int report_select(DevBuf &b, ResultHolder *R, int64_t nq, int64_t maxq, const int32_t *qlen,
                   const tpz_search_opts *o, const RankTables &rt, int64_t nh, int32_t *pprot,
                   int32_t *pgs, int32_t *pgl, int32_t *pso, int32_t *raw, int32_t *qend,
-                  int32_t *send, int32_t *psw, cudaEvent_t done) {
+                  int32_t *send, int32_t *psw, const HitPairs &hp, cudaEvent_t done) {
     const int top = o->report_hits;
     int npad = 1;
     while (npad < maxq) npad <<= 1;
@@ -385,6 +422,33 @@ int report_select(DevBuf &b, ResultHolder *R, int64_t nq, int64_t maxq, const in
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     rank_select_kernel<<<(unsigned)nq, kRankThreads, smem>>>(ra);
     offsets_kernel<<<1, 1024>>>(d_nsel, (int)nq, d_off);
+    if (hp.hit2pair) {
+        // the SW ran scores only: end coordinates of the reported hits
+        const int64_t ns = std::min<int64_t>(nh, nq * (int64_t)top);
+        SelPairArgs sp;
+        int64_t *lqo, *lso; int32_t *lql, *lsl, *lhit, *lcnt, *lsc, *lre, *lrd, *lst;
+        if ((rc = b.alloc(&lqo, ns)) || (rc = b.alloc(&lso, ns)) || (rc = b.alloc(&lql, ns)) ||
+            (rc = b.alloc(&lsl, ns)) || (rc = b.alloc(&lhit, ns)) || (rc = b.alloc(&lcnt, 1)) ||
+            (rc = b.alloc(&lsc, ns)) || (rc = b.alloc(&lre, ns)) || (rc = b.alloc(&lrd, ns)) ||
+            (rc = b.alloc(&lst, ns)))
+            return rc;
+        TPZ_CUDA(cudaMemset(lcnt, 0, 4));
+        sp.sel = d_sel; sp.nsel = d_nsel; sp.sw_status = psw; sp.hit2pair = hp.hit2pair;
+        sp.nq = (int)nq; sp.top = top; sp.pq_off = hp.pq_off; sp.ps_off = hp.ps_off;
+        sp.pq_len = hp.pq_len; sp.ps_len = hp.ps_len; sp.lq_off = lqo; sp.ls_off = lso;
+        sp.lq_len = lql; sp.ls_len = lsl; sp.lhit = lhit; sp.count = lcnt;
+        const int64_t tot = nq * (int64_t)top;
+        selected_pairs_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256>>>(sp);
+        int32_t nsp = 0;
+        TPZ_CUDA(cudaMemcpy(&nsp, lcnt, 4, cudaMemcpyDeviceToHost));
+        if (nsp > 0) {
+            rc = tpz::sw::batch_device_x(nsp, hp.q, lqo, lql, hp.T, lso, lsl, o->mat625, o->gap_open,
+                                         o->gap_extend, lsc, lre, lrd, lst, 0, hp.xmap, hp.xmap, 0);
+            if (rc) return rc;
+            scatter_sw_kernel<<<(unsigned)std::min<int64_t>((nsp + 255) / 256, 4096), 256>>>(
+                nsp, lhit, lsc, lre, lrd, lst, raw, send, qend, psw, nullptr);
+        }
+    }
     GatherArgs g;
     g.sel = d_sel; g.nsel = d_nsel; g.off = d_off; g.nq = (int)nq; g.top = top;
     const int32_t *src[kGatherFields] = {pprot, pgs, pgl, pso, raw, qend, send, psw};
@@ -722,14 +786,14 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
 
     if (nh > 0) {
         int64_t *dho, *pq_off, *ps_off; int32_t *pprot, *pgs, *pgl, *pso, *psw, *pq_len, *ps_len, *p_hit, *dnp;
-        int32_t *sc, *re, *rd, *st, *raw, *qend, *send;
+        int32_t *sc, *re, *rd, *st, *raw, *qend, *send, *hit2pair;
         if ((rc = b.alloc(&dho, nq + 1)) || (rc = b.alloc(&pprot, nh)) || (rc = b.alloc(&pgs, nh)) ||
             (rc = b.alloc(&pgl, nh)) || (rc = b.alloc(&pso, nh)) || (rc = b.alloc(&psw, nh)) ||
             (rc = b.alloc(&pq_off, nh)) || (rc = b.alloc(&ps_off, nh)) || (rc = b.alloc(&pq_len, nh)) ||
             (rc = b.alloc(&ps_len, nh)) || (rc = b.alloc(&p_hit, nh)) || (rc = b.alloc(&dnp, 1)) ||
             (rc = b.alloc(&sc, nh)) || (rc = b.alloc(&re, nh)) || (rc = b.alloc(&rd, nh)) ||
             (rc = b.alloc(&st, nh)) || (rc = b.alloc(&raw, nh)) || (rc = b.alloc(&qend, nh)) ||
-            (rc = b.alloc(&send, nh)))
+            (rc = b.alloc(&send, nh)) || (rc = b.alloc(&hit2pair, report ? nh : 1)))
             return bail(rc);
         if (cudaMemcpy(dho, R->hit_off.data(), 8 * (nq + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemset(dnp, 0, 4) != cudaSuccess || cudaMemset(raw, 0xFF, 4 * nh) != cudaSuccess ||
@@ -746,16 +810,23 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         if (cudaMemcpy(&npairs, dnp, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
             return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch pairs"));
         if (npairs > 0) {
+            // report mode ranks on scores alone: end coordinates come later,
+            // for the reported hits only
             rc = tpz::sw::batch_device_x(npairs, (const int8_t *)dq, pq_off, pq_len,
                                          (const int8_t *)ix->d.T, ps_off, ps_len, o->mat625,
-                                         o->gap_open, o->gap_extend, sc, re, rd, st, 0, xmap, xmap);
+                                         o->gap_open, o->gap_extend, sc, re, rd, st, 0, xmap, xmap,
+                                         report ? 1 : 0);
             if (rc) return bail(rc);
             scatter_sw_kernel<<<(unsigned)std::min<int64_t>((npairs + 255) / 256, 4096), 256>>>(
-                npairs, p_hit, sc, re, rd, st, raw, send, qend, psw);
+                npairs, p_hit, sc, re, rd, st, raw, send, qend, psw, report ? hit2pair : nullptr);
         }
         if (report) {
+            HitPairs hp;
+            hp.q = (const int8_t *)dq; hp.T = (const int8_t *)ix->d.T; hp.pq_off = pq_off;
+            hp.ps_off = ps_off; hp.pq_len = pq_len; hp.ps_len = ps_len;
+            hp.hit2pair = npairs > 0 ? hit2pair : nullptr; hp.xmap = xmap;
             int rc2 = report_select(b, R, nq, maxq, qlen, o, rt, nh, pprot, pgs, pgl, pso, raw, qend, send,
-                                    psw, ev[3]);
+                                    psw, hp, ev[3]);
             if (rc2) return bail(rc2);
         } else {
         if (cudaEventRecord(ev[3], 0) != cudaSuccess)

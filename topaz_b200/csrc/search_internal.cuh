@@ -95,11 +95,13 @@ __global__ void lower_bound_kernel(DevIndex ix, const uint8_t *pcat, const int64
 
 namespace sw {
 // Batched SW over device buffers; xq/xs (128-entry maps, may be null) turn
-// query/subject bytes into matrix indices inside the kernel.
+// query/subject bytes into matrix indices inside the kernel; score_only
+// skips the end coordinates (ref_end = read_end = -2 for TPZ_SW_OK pairs).
 int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
-                   int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs);
+                   int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
+                   int score_only);
 }  // namespace sw
 
 }  // namespace tpz

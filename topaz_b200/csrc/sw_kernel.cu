@@ -99,6 +99,7 @@ struct Args {
     int ssw_lanes;           // 16 (u8 pass) or 8 (i16 pass)
     int gap_open, gap_extend, bias;
     int translate;           // 1: q/s bytes go through xq/xs first
+    int score_only;          // 1: scores only, no end coordinates (ref_end = read_end = -2)
     uint32_t *bnd;           // stripe boundary rows, bnd_words per block (multi-stripe bins)
     int64_t bnd_words;
     int32_t *exact_list;     // i16-pass pairs near 32767: re-run in 32-bit arithmetic
@@ -320,7 +321,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             runmax = cm;
             cmx = cm;
         }
-        if (__any_sync(0xFFFFFFFFu, need)) {
+        if (!a.score_only && __any_sync(0xFFFFFFFFu, need)) {
             // smallest row holding the column maximum, both halves at once:
             // max(H - cm, -1) is 0 on rows holding it and -1 elsewhere; those
             // rows contribute R - r and the largest contribution wins
@@ -353,6 +354,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
         step(k + 1, wa2, wb2, wa, wb);
     }
 
+    if (a.score_only) { colA = colB = 0; rowA = rowB = 0; }
     kA = max(kA, best_key(lo16(runmax), colA, rowA));
     kB = max(kB, best_key(hi16(runmax), colB, rowB));
     __syncwarp();
@@ -381,8 +383,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
                 a.exact_list[slot] = p;
             } else {
                 a.score[p] = v;
-                a.ref_end[p] = col;
-                a.read_end[p] = row;
+                a.ref_end[p] = a.score_only ? -2 : col;
+                a.read_end[p] = a.score_only ? -2 : row;
                 a.status[p] = TPZ_SW_OK;
             }
         }
@@ -740,7 +742,8 @@ __global__ void __launch_bounds__(kExactThreads) sw_exact_kernel(const __grid_co
 int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
-                   int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs) {
+                   int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
+                   int score_only) {
     g_last_launches = 0;
     if (n < 0 || n > INT32_MAX / 3 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
     if (!(go > ge && ge >= 0 && go <= 255)) {
@@ -784,6 +787,7 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     a.bias = -mn;
     memcpy(a.mat, mat, 625);
     a.translate = (xq && xs) ? 1 : 0;
+    a.score_only = score_only;
     memset(a.xq, 0, sizeof a.xq);
     memset(a.xs, 0, sizeof a.xs);
     if (a.translate) {
@@ -832,7 +836,7 @@ int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t 
                  int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                  int32_t *status, cudaStream_t st) {
     return batch_device_x(n, q, qoff, qlen, s, soff, slen, mat, go, ge, score, ref_end, read_end,
-                          status, st, nullptr, nullptr);
+                          status, st, nullptr, nullptr, 0);
 }
 
 }  // namespace sw
@@ -1169,6 +1173,7 @@ extern "C" int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int
     a.bias = -mn;
     memcpy(a.mat, mat625_host, 625);
     a.translate = 0;
+    a.score_only = 0;
     memset(a.xq, 0, sizeof a.xq);
     memset(a.xs, 0, sizeof a.xs);
     a.bnd = nullptr;
