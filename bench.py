@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--search-workers", type=int, default=2,
                     help="host threads issuing search batches concurrently")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop section")
+    ap.add_argument("--search-proteins", type=int, default=1_000_000,
+                    help="DB size of the full-search section (proteins)")
+    ap.add_argument("--search-queries", type=int, default=10_000,
+                    help="queries of the full-search section")
     ap.add_argument("--search-batch", type=int, default=2500,
                     help="queries per tpz_search_batch call in the full-search section")
     ap.add_argument("--no-search", action="store_true",
@@ -221,11 +225,13 @@ def search_bench(args, dev):
     from topaz_b200 import build as B, dbformat, gpu_sa, native, synth
 
     t0 = time.perf_counter()
-    res, lens = synth.protein_db_arrays(1_000_000, seed=args.seed + 11)
+    res, lens = synth.protein_db_arrays(args.search_proteins, seed=args.seed + 11)
     db = dbformat.build_from_arrays(res, lens)
     db.SA = gpu_sa.suffix_array(db.T, dev)
     torch.cuda.empty_cache()
-    qres, qlens = synth.search_queries_arrays(res, lens, 5000, 5000, seed=args.seed + 12)
+    qres, qlens = synth.search_queries_arrays(res, lens, args.search_queries // 2,
+                                              args.search_queries - args.search_queries // 2,
+                                              seed=args.seed + 12)
     qoff = np.cumsum(qlens) - qlens
     q_aa = [qres[o:o + n].tobytes() for o, n in zip(qoff, qlens)]
     setup_s = time.perf_counter() - t0
@@ -264,7 +270,11 @@ def search_bench(args, dev):
         t.join()
     wall = time.perf_counter() - t0
     nh = nh[0]
-    out = {"workload": SEARCH_WORKLOAD % bsz, "queries": len(q_aa), "queries_per_s": round(len(q_aa) / wall, 1),
+    wl = SEARCH_WORKLOAD % bsz
+    if (args.search_proteins, args.search_queries) != (1_000_000, 10_000):
+        wl = ("smaller full search: %d-protein synthetic DB, %d queries (otherwise as the "
+              "mid-size config), batches of %d" % (args.search_proteins, args.search_queries, bsz))
+    out = {"workload": wl, "queries": len(q_aa), "queries_per_s": round(len(q_aa) / wall, 1),
            "wall_s": round(wall, 3),
            "api": "tpz_search_batch report mode (host buffers; SEG + alphabet on the host, "
                   "ranking and -H/-E cut on the device, all inside the timed region; "
@@ -389,22 +399,20 @@ def native_arm(args, rank, local_rank, world):
     dpx_ops_s = ops / (e0.elapsed_time(e1) / 1e3)
     peak_gcups = dpx_ops_s / DPX_OPS_PER_CELL / 1e9
 
-    for _ in range(args.warmup):
-        native.sw_batch_torch(t, mat, 11, 1)
-    torch.cuda.synchronize()
-    launches_per_step = native.last_launches()
-    status = t["status"].cpu().numpy()
-    assert (status == native.TPZ_SW_OK).all(), "pairs not aligned: %s" % np.unique(status)
-
     pr = torch.cuda.get_device_properties(dev)
     bus = "%08X:%02X:%02X.0" % (getattr(pr, "pci_domain_id", 0), getattr(pr, "pci_bus_id", 0),
                                 getattr(pr, "pci_device_id", 0))
     clocks = ClockSampler(bus or "")
-    barrier()
-    torch.cuda.synchronize()
     clocks.start()
-    time.sleep(0.3)
+    # warm-up right before the timed steps, so that the clocks do not idle
+    # down in between
+    barrier()
+    for _ in range(args.warmup):
+        native.sw_batch_torch(t, mat, 11, 1)
+    launches_per_step = native.last_launches()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.synchronize()
+    barrier()
     ev[0].record(stream)
     for i in range(args.steps):
         native.sw_batch_torch(t, mat, 11, 1)
@@ -412,6 +420,8 @@ def native_arm(args, rank, local_rank, world):
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
+    status = t["status"].cpu().numpy()
+    assert (status == native.TPZ_SW_OK).all(), "pairs not aligned: %s" % np.unique(status)
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     total_ms = sum(step_ms)
     tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
