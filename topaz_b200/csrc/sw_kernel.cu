@@ -164,6 +164,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     // into the high half
     constexpr uint32_t SEL[4] = {0xC480u, 0xD591u, 0xE6A2u, 0xF7B3u};
     uint64_t kA = 0, kB = 0;
+    bool decided = false;      // u8 pass: both pairs already go to the i16 pass
 
     // Queries longer than one stripe (32 lanes x R rows) run stripe after
     // stripe; the last row of a stripe (H, F, Fm per column) goes to `bnd`
@@ -260,6 +261,15 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
                 wm = __vimax_s16x2_relu(wm, __shfl_xor_sync(0xFFFFFFFFu, wm, o));
+            if (a.ssw_lanes == 16) {
+                // u8 pass: a pair whose maximum reached 255 - bias is decided
+                // (the i16 pass reruns it), so it needs no more row searches,
+                // and a task whose pairs are both decided stops here
+                const bool da = lo16(wm) + a.bias >= 255, db = hi16(wm) + a.bias >= 255;
+                if (da) wm = (wm & 0xFFFF0000u) | 0x7FFFu;
+                if (db) wm = (wm & 0x0000FFFFu) | 0x7FFF0000u;
+                if (da && (db || pB < 0)) decided = true;
+            }
             wmax = wm;
             __syncwarp();
         }
@@ -349,15 +359,16 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     uint32_t wa2[W], wb2[W];
     // an even step count; a step past N + 30 finds every lane past the end
     const int steps = (N + 32) & ~1;
-    for (int k = 0; k < steps; k += 2) {
+    for (int k = 0; k < steps && !decided; k += 2) {
         step(k, wa, wb, wa2, wb2);
         step(k + 1, wa2, wb2, wa, wb);
     }
 
-    if (a.score_only) { colA = colB = 0; rowA = rowB = 0; }
+    if (a.score_only || decided) { colA = colB = 0; rowA = rowB = 0; }
     kA = max(kA, best_key(lo16(runmax), colA, rowA));
     kB = max(kB, best_key(hi16(runmax), colB, rowB));
     __syncwarp();
+    if (decided) break;
     }   // stripes
 
     // ---- warp reduction: max value, then first column, then smallest row
