@@ -240,9 +240,20 @@ def search_bench(args, dev):
     load_s = time.perf_counter() - t0
     mat = synth.matrix("BLOSUM62")
     report = {"max_evalue": 1e-3}                     # -H 100 -E 1e-3, ranked on the device
-    ix.search([native.prepare_query(q) for q in q_aa[:200]], mat, report=report)   # warm-up
-    torch.cuda.synchronize()
     bsz = args.search_batch
+    # warm-up: one full-size batch per worker thread, so that the device
+    # memory pool of every thread has grown to a batch before the timing
+    warm = [native.prepare_query(q) for q in q_aa[:bsz]]
+
+    def warm_one():
+        ix.search(warm, mat, report=report)
+
+    th = [threading.Thread(target=warm_one) for _ in range(args.search_workers)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    torch.cuda.synchronize()
     stage = np.zeros(4)
     nh = [0]
     starts = list(range(0, len(q_aa), bsz))

@@ -103,14 +103,33 @@ struct PackArgs {
     // SW pairs
     int64_t *pq_off, *ps_off;
     int32_t *pq_len, *ps_len, *p_hit;
-    int32_t *npairs;
+    const int64_t *pair_off;  // nq + 1: the SW pairs of query q start at pair_off[q]
 };
 
-// packs the per-query hit lists and lists the SW pairs (gapless >= 40)
+// SW pairs (hits with gapless score >= 40) per query
+__global__ void count_pairs_kernel(PackArgs a, int32_t *cnt) {
+    __shared__ int c;
+    const int q = blockIdx.x;
+    const int n = a.qout[q].nhits;
+    if (threadIdx.x == 0) c = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int h = threadIdx.x; h < n; h += blockDim.x)
+        mine += a.hits[(int64_t)q * a.max_cap + h].gapless_score >= 40;
+    if (mine) atomicAdd(&c, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) cnt[q] = c;
+}
+
+// packs the per-query hit lists and lists the SW pairs (gapless >= 40),
+// the pairs of a query together
 __global__ void pack_hits_kernel(PackArgs a) {
+    __shared__ int k0;
     const int q = blockIdx.x;
     const int n = a.qout[q].nhits;
     const int64_t base = a.hit_off[q];
+    if (threadIdx.x == 0) k0 = 0;
+    __syncthreads();
     for (int h = threadIdx.x; h < n; h += blockDim.x) {
         const Hit x = a.hits[(int64_t)q * a.max_cap + h];
         const int64_t o = base + h;
@@ -121,7 +140,7 @@ __global__ void pack_hits_kernel(PackArgs a) {
         if (x.gapless_score < 40) {
             a.sw_status[o] = TPZ_SW_GAPLESS_LOW;
         } else {
-            const int k = atomicAdd(a.npairs, 1);
+            const int64_t k = a.pair_off[q] + atomicAdd(&k0, 1);
             a.pq_off[k] = a.qoff[q];
             a.pq_len[k] = a.qlen[q];
             a.ps_off[k] = a.pstart[x.protein];
@@ -785,18 +804,19 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     for (int64_t q = 0; q < nq; ++q) maxq = std::max<int64_t>(maxq, qo[q].nhits);
 
     if (nh > 0) {
-        int64_t *dho, *pq_off, *ps_off; int32_t *pprot, *pgs, *pgl, *pso, *psw, *pq_len, *ps_len, *p_hit, *dnp;
+        int64_t *dho, *pq_off, *ps_off, *dpoff; int32_t *pprot, *pgs, *pgl, *pso, *psw, *pq_len, *ps_len, *p_hit, *dnp;
         int32_t *sc, *re, *rd, *st, *raw, *qend, *send, *hit2pair;
         if ((rc = b.alloc(&dho, nq + 1)) || (rc = b.alloc(&pprot, nh)) || (rc = b.alloc(&pgs, nh)) ||
             (rc = b.alloc(&pgl, nh)) || (rc = b.alloc(&pso, nh)) || (rc = b.alloc(&psw, nh)) ||
             (rc = b.alloc(&pq_off, nh)) || (rc = b.alloc(&ps_off, nh)) || (rc = b.alloc(&pq_len, nh)) ||
-            (rc = b.alloc(&ps_len, nh)) || (rc = b.alloc(&p_hit, nh)) || (rc = b.alloc(&dnp, 1)) ||
+            (rc = b.alloc(&ps_len, nh)) || (rc = b.alloc(&p_hit, nh)) || (rc = b.alloc(&dnp, nq)) ||
+            (rc = b.alloc(&dpoff, nq + 1)) ||
             (rc = b.alloc(&sc, nh)) || (rc = b.alloc(&re, nh)) || (rc = b.alloc(&rd, nh)) ||
             (rc = b.alloc(&st, nh)) || (rc = b.alloc(&raw, nh)) || (rc = b.alloc(&qend, nh)) ||
             (rc = b.alloc(&send, nh)) || (rc = b.alloc(&hit2pair, report ? nh : 1)))
             return bail(rc);
         if (cudaMemcpy(dho, R->hit_off.data(), 8 * (nq + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(dnp, 0, 4) != cudaSuccess || cudaMemset(raw, 0xFF, 4 * nh) != cudaSuccess ||
+            cudaMemset(raw, 0xFF, 4 * nh) != cudaSuccess ||
             cudaMemset(qend, 0xFF, 4 * nh) != cudaSuccess || cudaMemset(send, 0xFF, 4 * nh) != cudaSuccess)
             return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch pack"));
         PackArgs pa;
@@ -804,18 +824,22 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         pa.pstart = ix->d.pstart; pa.nq = (int)nq; pa.max_cap = max_cap;
         pa.protein = pprot; pa.gs = pgs; pa.gl = pgl; pa.so = pso; pa.sw_status = psw;
         pa.pq_off = pq_off; pa.ps_off = ps_off; pa.pq_len = pq_len; pa.ps_len = ps_len;
-        pa.p_hit = p_hit; pa.npairs = dnp;
+        pa.p_hit = p_hit; pa.pair_off = dpoff;
+        count_pairs_kernel<<<(unsigned)nq, 256>>>(pa, dnp);
+        offsets_kernel<<<1, 1024>>>(dnp, (int)nq, dpoff);
         pack_hits_kernel<<<(unsigned)nq, 256>>>(pa);
-        int32_t npairs = 0;
-        if (cudaMemcpy(&npairs, dnp, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        std::vector<int64_t> poff(nq + 1);
+        if (cudaMemcpy(poff.data(), dpoff, 8 * (nq + 1), cudaMemcpyDeviceToHost) != cudaSuccess)
             return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch pairs"));
+        const int64_t npairs = poff[nq];
         if (npairs > 0) {
-            // report mode ranks on scores alone: end coordinates come later,
-            // for the reported hits only
-            rc = tpz::sw::batch_device_x(npairs, (const int8_t *)dq, pq_off, pq_len,
-                                         (const int8_t *)ix->d.T, ps_off, ps_len, o->mat625,
-                                         o->gap_open, o->gap_extend, sc, re, rd, st, 0, xmap, xmap,
-                                         report ? 1 : 0);
+            // the pairs of a query share its profile; report mode ranks on
+            // scores alone (end coordinates come later, for the reported hits)
+            rc = tpz::sw::batch_device_grouped(npairs, (const int8_t *)dq, pq_off, pq_len,
+                                               (const int8_t *)ix->d.T, ps_off, ps_len, o->mat625,
+                                               o->gap_open, o->gap_extend, sc, re, rd, st, 0, xmap,
+                                               xmap, report ? 1 : 0, nq, dpoff, poff.data(),
+                                               qlen_eff.data());
             if (rc) return bail(rc);
             scatter_sw_kernel<<<(unsigned)std::min<int64_t>((npairs + 255) / 256, 4096), 256>>>(
                 npairs, p_hit, sc, re, rd, st, raw, send, qend, psw, report ? hit2pair : nullptr);

@@ -101,7 +101,17 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
-                   int score_only);
+                   int score_only, const int32_t *subset = nullptr, int64_t nsub = 0);
+// The same for pairs grouped by query (group g = pairs [gstart[g],
+// gstart[g+1]), all with query length gqlen[g]): groups with enough pairs go
+// to the query-major kernels, one shared profile per query; the rest by pair.
+int batch_device_grouped(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                         const int8_t *s, const int64_t *soff, const int32_t *slen,
+                         const int8_t *mat, int go, int ge, int32_t *score, int32_t *ref_end,
+                         int32_t *read_end, int32_t *status, cudaStream_t st, const int8_t *xq,
+                         const int8_t *xs, int score_only, int64_t ngroups,
+                         const int64_t *gstart_dev, const int64_t *gstart_host,
+                         const int32_t *gqlen_host);
 }  // namespace sw
 
 }  // namespace tpz

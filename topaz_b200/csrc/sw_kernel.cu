@@ -139,10 +139,15 @@ __device__ __forceinline__ uint32_t letter_pair(const Args &a, const int8_t *sA,
     return (uint32_t)la | ((uint32_t)lb << 8);
 }
 
-template <int R, bool MULTI>
+// One task: pairs pA and pB (pB < 0: none) in the halves of the int16x2
+// lanes.  lanes = 16 (u8 pass) or 8 (i16 pass); u8 results that saturate go
+// to rerun[atomicAdd(rerun_count)].  BUILD = false: profA/profB already hold
+// the query profiles (both pairs then share one query).
+template <int R, bool MULTI, bool BUILD = true>
 __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
                                          uint32_t *profA, uint32_t *profB, uint16_t *ring,
-                                         int stripes, uint32_t *bnd) {
+                                         int stripes, uint32_t *bnd, int lanes, int32_t *rerun,
+                                         int32_t *rerun_count) {
     constexpr int W = words_for(R);
     const int lane = threadIdx.x & 31;
 
@@ -155,8 +160,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     const int8_t *qB = pB >= 0 ? a.q + a.qoff[pB] : qA;
     const int8_t *sB = pB >= 0 ? a.s + a.soff[pB] : sA;
     const int N = max(slA, slB);
-    const int segA = max(1, (qlA + a.ssw_lanes - 1) / a.ssw_lanes);
-    const int segB = max(1, (qlB + a.ssw_lanes - 1) / a.ssw_lanes);
+    const int segA = max(1, (qlA + lanes - 1) / lanes);
+    const int segB = max(1, (qlB + lanes - 1) / lanes);
     const uint32_t NGO = pack2(-a.gap_open, -a.gap_open);
     const uint32_t NGE = pack2(-a.gap_extend, -a.gap_extend);
     const uint32_t NEGINF = 0x80008000u;
@@ -176,6 +181,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
 
     // ---- profile of this lane's rows for all 26 letters (25 + pad column),
     // word w of letter l at [(l * W + w) * 32 + lane]: conflict-free per lane
+    if constexpr (BUILD) {
     int qa[R], qb[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -209,6 +215,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             profB[(let * W + w) * 32 + lane] = wb;
         }
     }
+    }   // BUILD
     // ---- subject letters: columns 0..63 in the ring, 64..95 in flight;
     // every 32 steps the lanes store the next 32 columns and fetch 32 more
     ring[lane] = (uint16_t)letter_pair(a, sA, slA, sB, slB, lane);
@@ -261,7 +268,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
                 wm = __vimax_s16x2_relu(wm, __shfl_xor_sync(0xFFFFFFFFu, wm, o));
-            if (a.ssw_lanes == 16) {
+            if (lanes == 16) {
                 // u8 pass: a pair whose maximum reached 255 - bias is decided
                 // (the i16 pass reruns it), so it needs no more row searches,
                 // and a task whose pairs are both decided stops here
@@ -384,11 +391,11 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             const int v = (int)(key >> 40);
             const int col = key ? 0xFFFFFF - (int)((key >> 16) & 0xFFFFFF) : -1;
             const int row = key ? 0xFFFF - (int)(key & 0xFFFF) : 0;
-            if (a.ssw_lanes == 16 && v + a.bias >= 255) {
+            if (lanes == 16 && v + a.bias >= 255) {
                 // u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
-                const int slot = atomicAdd(a.rerun_count, 1);
-                a.rerun[slot] = p;
-            } else if (a.ssw_lanes == 8 && a.exact_list && v >= a.exact_threshold) {
+                const int slot = atomicAdd(rerun_count, 1);
+                rerun[slot] = p;
+            } else if (lanes == 8 && a.exact_list && v >= a.exact_threshold) {
                 // near the i16 limit: 16-bit lanes may wrap, redo in 32 bits
                 const int slot = atomicAdd(a.exact_count, 1);
                 a.exact_list[slot] = p;
@@ -431,11 +438,13 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
         if constexpr (R == kMaxR) {
             if (stripes > 1) {
                 run_task<R, true>(a, pA, pB, smat, profA, profB, ring, stripes,
-                                  a.bnd + (size_t)blockIdx.x * a.bnd_words);
+                                  a.bnd + (size_t)blockIdx.x * a.bnd_words, a.ssw_lanes, a.rerun,
+                                  a.rerun_count);
                 continue;
             }
         }
-        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr);
+        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr, a.ssw_lanes, a.rerun,
+                           a.rerun_count);
     }
 }
 
@@ -463,12 +472,148 @@ __global__ void __launch_bounds__(32) sw_one_kernel(const __grid_constant__ Args
     b.qoff = &s_off; b.soff = &s_off; b.qlen = &s_ql; b.slen = &s_sl;
     b.rerun_count = &s_rr[0]; b.rerun = &s_rr[1];
     b.ssw_lanes = 16;
-    run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr);
+    run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr, 16, b.rerun, b.rerun_count);
     __syncwarp();
     if (s_rr[0]) {
         // the u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
         b.ssw_lanes = 8;
-        run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr);
+        run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr, 8, b.rerun, b.rerun_count);
+    }
+}
+
+// ------------------------------------------------------------- query-major
+
+// Pairs that share their query (the hits of one search query): a block of
+// kQmWarps warps per query keeps ONE profile of the query in shared memory
+// for all of them, so a warp costs the SM a fraction of the shared memory
+// of the pair-per-task kernel and more warps hide the DPX latency.  The
+// block sorts the query's pairs by subject length (longest first, two per
+// task), runs the u8 pass over all of them and then, with the profile
+// still resident, the i16 pass over those that saturated.
+constexpr int kQmWarps = 8;
+constexpr int kQmMaxPairs = 256;      // pairs per chunk: longer pair lists of a query are cut
+constexpr int kQmMinPairs = 2 * kQmWarps;
+constexpr int kQmStreams = 8;
+
+__host__ __device__ constexpr int qm_smem_bytes(int R) {
+    return kSmatBytes + profile_bytes(R) + kQmWarps * 2 * kRing + 8 * kQmMaxPairs +
+           4 * kQmMaxPairs;
+}
+
+struct QmArgs {
+    const int64_t *chunks;    // [first pair, end) per chunk; the pairs of a chunk share the query
+    const int32_t *bin_info;  // per row bin R-1: [first chunk, count]
+    int32_t *next;            // per row bin: chunk counter
+};
+
+// profile words of letters warp, warp + kQmWarps, ... for lane's rows of the
+// query of pair p
+template <int R>
+__device__ __forceinline__ void qm_build_profile(const Args &a, int64_t p, const int8_t *smat,
+                                                 uint32_t *prof, int warp, int lane) {
+    constexpr int W = words_for(R);
+    const int ql = a.qlen[p];
+    const int8_t *qp = a.q + a.qoff[p];
+    const int i0 = lane * R;
+    int qv[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        int x = (i0 + r < ql) ? qp[i0 + r] : -1;
+        if (a.translate && x >= 0) x = a.xq[x & 127];
+        qv[r] = (x >= 25) ? -1 : x;
+    }
+    for (int let = warp; let < 26; let += kQmWarps) {
+        const int8_t *mrow = smat + let * kMatStride;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int r = 4 * w + k;
+                int v = kPadScore;
+                if (r < R && qv[r] >= 0) v = mrow[qv[r]];
+                word |= (uint32_t)(uint8_t)(int8_t)v << (8 * k);
+            }
+            prof[(let * W + w) * 32 + lane] = word;
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(kQmWarps * 32) sw_query_kernel(const __grid_constant__ Args a,
+                                                                 QmArgs g, int bin) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    int8_t *smat = reinterpret_cast<int8_t *>(smem);
+    uint32_t *prof = reinterpret_cast<uint32_t *>(smem + kSmatBytes);
+    uint16_t *rings = reinterpret_cast<uint16_t *>(prof + profile_bytes(R) / 4);
+    uint64_t *keys = reinterpret_cast<uint64_t *>(rings + kQmWarps * kRing);
+    int32_t *sat = reinterpret_cast<int32_t *>(keys + kQmMaxPairs);
+    __shared__ int s_group, s_next, s_nsat;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint16_t *ring = rings + warp * kRing;
+    const int gb = g.bin_info[2 * bin], gc = g.bin_info[2 * bin + 1];
+    if (gc == 0) return;
+    for (int i = threadIdx.x; i < 26 * kMatStride; i += blockDim.x) {
+        const int r = i / kMatStride, c = i % kMatStride;
+        smat[i] = (r < 25 && c < 25) ? a.mat[r * 25 + c] : (int8_t)kPadScore;
+    }
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_group = atomicAdd(&g.next[bin], 1);
+            s_next = 0;
+            s_nsat = 0;
+        }
+        __syncthreads();
+        if (s_group >= gc) break;
+        const int64_t p0 = g.chunks[2 * (gb + s_group)];
+        const int n = (int)(g.chunks[2 * (gb + s_group) + 1] - p0);
+        int np = 1;
+        while (np < n) np <<= 1;
+        // keys: subject length + 1 (descending), pair id; padding 0 sorts last
+        for (int i = threadIdx.x; i < np; i += blockDim.x)
+            keys[i] = i < n ? ((uint64_t)(uint32_t)(a.slen[p0 + i] + 1) << 32) | (uint32_t)(p0 + i)
+                            : 0ull;
+        qm_build_profile<R>(a, p0, smat, prof, warp, lane);
+        __syncthreads();
+        for (int k = 2; k <= np; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < np; i += blockDim.x) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const uint64_t x = keys[i], y = keys[l];
+                        if (((i & k) == 0) ? (x < y) : (x > y)) { keys[i] = y; keys[l] = x; }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // u8 pass over every pair of the query
+        for (;;) {
+            int t = 0;
+            if (lane == 0) t = atomicAdd(&s_next, 1);
+            t = __shfl_sync(0xFFFFFFFFu, t, 0);
+            if (2 * t >= n) break;
+            const int pA = (int)(uint32_t)keys[2 * t];
+            const int pB = 2 * t + 1 < n ? (int)(uint32_t)keys[2 * t + 1] : -1;
+            run_task<R, false, false>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 16, sat,
+                                      &s_nsat);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = 0;
+        __syncthreads();
+        // i16 pass over the pairs that saturated (src/ssw.c:863-865)
+        const int ns = s_nsat;
+        for (;;) {
+            int t = 0;
+            if (lane == 0) t = atomicAdd(&s_next, 1);
+            t = __shfl_sync(0xFFFFFFFFu, t, 0);
+            if (2 * t >= ns) break;
+            const int pA = sat[2 * t];
+            const int pB = 2 * t + 1 < ns ? sat[2 * t + 1] : -1;
+            run_task<R, false, false>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 8, nullptr,
+                                      nullptr);
+        }
     }
 }
 
@@ -498,6 +643,8 @@ __global__ void bin_count_kernel(int64_t n, const int32_t *list, const int32_t *
         if (ql > kStripeRows && multi_maxn) atomicMax(multi_maxn, sl);
     }
 }
+
+__global__ void set_i32_kernel(int32_t *p, int32_t v) { *p = v; }
 
 // one block of 1024 threads: exclusive scan of kBins counts -> cursor; the
 // per-R-bin [start, count] pairs -> rinfo; task counters cleared.
@@ -754,8 +901,9 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
-                   int score_only) {
+                   int score_only, const int32_t *subset, int64_t nsub) {
     g_last_launches = 0;
+    if (subset && nsub == 0) return TPZ_OK;
     if (n < 0 || n > INT32_MAX / 3 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
     if (!(go > ge && ge >= 0 && go <= 255)) {
         set_error("tpz_sw_batch: requires 255 >= gap_open > gap_extend >= 0");
@@ -813,10 +961,18 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
 
     int64_t launches = 0;
     int host_maxn = 0;
-    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, 3 * sizeof(int32_t), st));
+    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, 4 * sizeof(int32_t), st));
     a.ssw_lanes = 16;
-    rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, multi_maxn, st,
-                      launches, &host_maxn);
+    if (subset) {
+        // the first round over the given pair ids only
+        int32_t *d_nsub = rerun_count + 3;
+        set_i32_kernel<<<1, 1, 0, st>>>(d_nsub, (int32_t)nsub);
+        rc = launch_round(cfg, a, nsub, subset, d_nsub, counts, cursor, sorted, multi_maxn, st,
+                          launches, &host_maxn);
+    } else {
+        rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, multi_maxn, st,
+                          launches, &host_maxn);
+    }
     if (rc) { if (a.bnd) cudaFreeAsync(a.bnd, st); cudaFreeAsync(ws, st); return rc; }
     a.ssw_lanes = 8;
     rc = launch_round(cfg, a, n, rerun, rerun_count, counts, cursor, sorted, multi_maxn, st,
@@ -842,12 +998,209 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     return TPZ_OK;
 }
 
+// Per host thread and device: launch attributes of the query-major kernels
+// and two streams of their own, so that they run beside the pair-per-task
+// kernels of the same call.
+struct QmCfg {
+    typedef void (*Fn)(const Args, QmArgs, int);
+    Fn fn[kMaxR];
+    int blocks_per_sm[kMaxR];
+    cudaStream_t aux[kQmStreams];
+    cudaEvent_t fork, join[kQmStreams];
+};
+
+template <int R>
+struct QmTable {
+    static void fill(QmCfg::Fn *k) {
+        k[R - 1] = sw_query_kernel<R>;
+        QmTable<R - 1>::fill(k);
+    }
+};
+template <>
+struct QmTable<0> {
+    static void fill(QmCfg::Fn *) {}
+};
+
+struct QmCfgs {
+    std::vector<QmCfg *> per_dev;
+    ~QmCfgs() {
+        for (QmCfg *c : per_dev) {
+            if (!c) continue;
+            for (int i = 0; i < kQmStreams; ++i) { cudaStreamDestroy(c->aux[i]); cudaEventDestroy(c->join[i]); }
+            cudaEventDestroy(c->fork);
+            delete c;
+        }
+    }
+};
+
+static int qm_cfg(const QmCfg **out) {
+    static thread_local QmCfgs cfgs;
+    int dev = 0;
+    TPZ_CUDA(cudaGetDevice(&dev));
+    if ((int)cfgs.per_dev.size() <= dev) cfgs.per_dev.resize(dev + 1, nullptr);
+    if (!cfgs.per_dev[dev]) {
+        QmCfg *c = new QmCfg();
+        QmTable<kMaxR>::fill(c->fn);
+        for (int r = 1; r <= kMaxR; ++r) {
+            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          qm_smem_bytes(r)));
+            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
+                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared));
+            int nb = 0;
+            TPZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)c->fn[r - 1],
+                                                                   kQmWarps * 32, qm_smem_bytes(r)));
+            c->blocks_per_sm[r - 1] = std::max(1, nb);
+        }
+        for (int i = 0; i < kQmStreams; ++i) {
+            TPZ_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
+            TPZ_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
+        }
+        TPZ_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+        cfgs.per_dev[dev] = c;
+    }
+    *out = cfgs.per_dev[dev];
+    return TPZ_OK;
+}
+
+int batch_device_grouped(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
+                         const int8_t *s, const int64_t *soff, const int32_t *slen,
+                         const int8_t *mat, int go, int ge, int32_t *score, int32_t *ref_end,
+                         int32_t *read_end, int32_t *status, cudaStream_t st, const int8_t *xq,
+                         const int8_t *xs, int score_only, int64_t ngroups,
+                         const int64_t *gstart_dev, const int64_t *gstart_host,
+                         const int32_t *gqlen_host) {
+    if (n <= 0) return TPZ_OK;
+    if (!(go > ge && ge >= 0 && go <= 255) || !mat) {
+        set_error("tpz_sw_batch: requires 255 >= gap_open > gap_extend >= 0");
+        return TPZ_E_ARG;
+    }
+    // chunks of at most kQmMaxPairs pairs of one query for the query-major
+    // kernels (queries with enough pairs and one stripe); every other pair
+    // goes by pair
+    std::vector<std::vector<int64_t>> per_r(kMaxR);
+    std::vector<int64_t> work(kMaxR, 0);
+    std::vector<int32_t> rest;
+    for (int64_t g = 0; g < ngroups; ++g) {
+        const int64_t c = gstart_host[g + 1] - gstart_host[g];
+        if (c <= 0) continue;
+        const int ql = gqlen_host[g];
+        if (ql >= 1 && ql <= kStripeRows && c >= kQmMinPairs) {
+            const int64_t nch = (c + kQmMaxPairs - 1) / kQmMaxPairs;
+            for (int64_t i = 0; i < nch; ++i) {
+                // equal cuts so that no chunk is much smaller than the others
+                per_r[(ql + 31) / 32 - 1].push_back(gstart_host[g] + c * i / nch);
+                per_r[(ql + 31) / 32 - 1].push_back(gstart_host[g] + c * (i + 1) / nch);
+            }
+            work[(ql + 31) / 32 - 1] += c * ql;
+        } else {
+            for (int64_t k = gstart_host[g]; k < gstart_host[g + 1]; ++k) rest.push_back((int32_t)k);
+        }
+    }
+    std::vector<int64_t> chunks;
+    std::vector<int32_t> bin_info(2 * kMaxR, 0);
+    for (int r = 0; r < kMaxR; ++r) {
+        bin_info[2 * r] = (int32_t)(chunks.size() / 2);
+        bin_info[2 * r + 1] = (int32_t)(per_r[r].size() / 2);
+        chunks.insert(chunks.end(), per_r[r].begin(), per_r[r].end());
+    }
+    const QmCfg *qc = nullptr;
+    int rc = qm_cfg(&qc);
+    if (rc) return rc;
+    int64_t *dchunks = nullptr;
+    int32_t *dbin = nullptr, *dnext = nullptr, *drest = nullptr, *dexact = nullptr,
+            *dexact_n = nullptr;
+    auto cleanup = [&]() {
+        for (void *p : {(void *)dchunks, (void *)dbin, (void *)dnext, (void *)drest, (void *)dexact,
+                        (void *)dexact_n})
+            if (p) cudaFreeAsync(p, st);
+    };
+    if (cudaMallocAsync((void **)&dchunks, 8 * std::max<size_t>(chunks.size(), 1), st) ||
+        cudaMallocAsync((void **)&dbin, 4 * 2 * kMaxR, st) ||
+        cudaMallocAsync((void **)&dnext, 4 * kMaxR, st) ||
+        cudaMallocAsync((void **)&drest, 4 * std::max<size_t>(rest.size(), 1), st) ||
+        cudaMallocAsync((void **)&dexact, 4 * std::max<int64_t>(n, 1), st) ||
+        cudaMallocAsync((void **)&dexact_n, 4, st)) {
+        cleanup();
+        return cuda_fail(cudaGetLastError(), "batch_device_grouped");
+    }
+    if (cudaMemcpyAsync(dchunks, chunks.data(), 8 * chunks.size(), cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(dbin, bin_info.data(), 4 * 2 * kMaxR, cudaMemcpyHostToDevice, st) ||
+        cudaMemsetAsync(dnext, 0, 4 * kMaxR, st) || cudaMemsetAsync(dexact_n, 0, 4, st) ||
+        (rest.size() && cudaMemcpyAsync(drest, rest.data(), 4 * rest.size(), cudaMemcpyHostToDevice, st))) {
+        cleanup();
+        return cuda_fail(cudaGetLastError(), "batch_device_grouped copies");
+    }
+    Args a;
+    memset(&a, 0, sizeof a);
+    a.q = q; a.qoff = qoff; a.qlen = qlen; a.s = s; a.soff = soff; a.slen = slen;
+    a.score = score; a.ref_end = ref_end; a.read_end = read_end; a.status = status;
+    a.gap_open = go; a.gap_extend = ge;
+    int mn = 0, mx = 0;
+    for (int i = 0; i < 625; ++i) { mn = std::min<int>(mn, mat[i]); mx = std::max<int>(mx, mat[i]); }
+    a.bias = -mn;
+    memcpy(a.mat, mat, 625);
+    a.translate = (xq && xs) ? 1 : 0;
+    if (a.translate) { memcpy(a.xq, xq, 128); memcpy(a.xs, xs, 128); }
+    a.score_only = score_only;
+    a.exact_list = dexact;
+    a.exact_count = dexact_n;
+    a.exact_threshold = std::min(32767 - 2 * std::max(mx, 1), kBig);
+    QmArgs g;
+    g.chunks = dchunks; g.bin_info = dbin; g.next = dnext;
+    const int nsm = sm_count();
+    int64_t launches = 0;
+    if (!chunks.empty()) {
+        // one persistent kernel per row bin, the bins with the most work
+        // first, over kQmStreams streams so that bins share the SMs
+        TPZ_CUDA(cudaEventRecord(qc->fork, st));
+        for (int i = 0; i < kQmStreams; ++i) TPZ_CUDA(cudaStreamWaitEvent(qc->aux[i], qc->fork, 0));
+        std::vector<int> order;
+        for (int r = 1; r <= kMaxR; ++r) if (!per_r[r - 1].empty()) order.push_back(r);
+        std::sort(order.begin(), order.end(), [&](int x, int y) { return work[x - 1] > work[y - 1]; });
+        int k = 0;
+        for (int r : order) {
+            const int grid = (int)std::min<int64_t>((int64_t)nsm * qc->blocks_per_sm[r - 1],
+                                                    (int64_t)per_r[r - 1].size() / 2);
+            qc->fn[r - 1]<<<grid, kQmWarps * 32, qm_smem_bytes(r), qc->aux[k++ % kQmStreams]>>>(
+                a, g, r - 1);
+            ++launches;
+        }
+    }
+    rc = batch_device_x(n, q, qoff, qlen, s, soff, slen, mat, go, ge, score, ref_end, read_end,
+                        status, st, xq, xs, score_only, drest, (int64_t)rest.size());
+    launches += g_last_launches;
+    if (!chunks.empty()) {
+        for (int i = 0; i < kQmStreams; ++i) {
+            TPZ_CUDA(cudaEventRecord(qc->join[i], qc->aux[i]));
+            TPZ_CUDA(cudaStreamWaitEvent(st, qc->join[i], 0));
+        }
+        if (rc == TPZ_OK && (int64_t)kStripeRows * mx >= a.exact_threshold) {
+            int32_t *scratch = nullptr;
+            rc = cudaMallocAsync((void **)&scratch,
+                                 sizeof(int32_t) * 2 * (size_t)TPZ_SW_MAX_QLEN * kExactThreads, st)
+                     == cudaSuccess ? TPZ_OK : cuda_fail(cudaGetLastError(), "exact scratch");
+            if (rc == TPZ_OK) {
+                sw_exact_kernel<<<1, kExactThreads, 0, st>>>(a, scratch);
+                ++launches;
+                cudaFreeAsync(scratch, st);
+            }
+        }
+    }
+    cleanup();
+    if (rc) return rc;
+    TPZ_CUDA(cudaGetLastError());
+    g_last_launches = launches;
+    return TPZ_OK;
+}
+
 int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t *qlen,
                  const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                  int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                  int32_t *status, cudaStream_t st) {
     return batch_device_x(n, q, qoff, qlen, s, soff, slen, mat, go, ge, score, ref_end, read_end,
-                          status, st, nullptr, nullptr, 0);
+                          status, st, nullptr, nullptr, 0, nullptr, 0);
 }
 
 }  // namespace sw
