@@ -216,6 +216,14 @@ TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_
                              tpz_search_result **out);
 TPZ_API void tpz_search_result_free(tpz_search_result *r);
 
+/* Suffix array of the .psq bytes T[0, n) on the device, for `topaz index`
+ * (serif_index / create_index, src/index.c:24-93, build it on the host):
+ * SA[0, n) (host) receives the suffixes in byte-lexicographic order, a
+ * shorter suffix before a longer one with the same prefix -- the bytes of the
+ * reference's .SA file.  rounds (may be NULL) receives the number of sorting
+ * rounds.  n must be below 2^32 - 1 (TPZ_E_RANGE otherwise). */
+TPZ_API int tpz_sa_build(const uint8_t *T, int64_t n, int64_t *SA, int32_t *rounds);
+
 /* bitscore and E-value of a raw score exactly as align_using_ssw_profile
  * computes them with the C library's log/exp (src/ssw_wrapper.c:179-183,
  * :239-242); db_size = Tsize - Psize and db_proteins = Psize unless given

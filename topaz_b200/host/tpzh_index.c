@@ -12,6 +12,7 @@
  */
 #define _GNU_SOURCE
 #include "tpzh.h"
+#include "../../include/topaz_b200.h"
 
 #include <errno.h>
 #include <inttypes.h>
@@ -76,9 +77,15 @@ int tpzh_index(const char *fasta, const char *prefix) {
     fprintf(stderr, "mmapped T (%s), file size is %" PRId64 " bytes\n", tn, Tsize);
     free(tn);
     int64_t *SA = malloc(sizeof(int64_t) * (Tsize > 0 ? Tsize : 1));
-    if (!SA || tpzh_suffix_array(T, Tsize, SA) != 0) {
-        fprintf(stderr, "suffix array construction failed\n");
-        return -1;
+    if (!SA) { fprintf(stderr, "suffix array construction failed\n"); return -1; }
+    /* on the GPU (prefix doubling); the host SA-IS when there is none or
+     * the text is too long for it -- both give the same array */
+    if (tpz_sa_build(T, Tsize, SA, NULL) != 0) {
+        fprintf(stderr, "GPU suffix array unavailable (%s); building it on the host\n", tpz_last_error());
+        if (tpzh_suffix_array(T, Tsize, SA) != 0) {
+            fprintf(stderr, "suffix array construction failed\n");
+            return -1;
+        }
     }
     FILE *sa = open_w(prefix, ".SA");
     if (!sa || fwrite(SA, sizeof(int64_t), Tsize, sa) != (size_t)Tsize) return -1;
