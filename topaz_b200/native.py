@@ -118,6 +118,16 @@ def sw_align_one(q_ptr, qlen, s_ptr, slen, mat, gap_open, gap_extend, out4_ptr, 
                              gap_open, gap_extend, out4_ptr, stream))
 
 
+def sa_build(T) -> np.ndarray:
+    """Suffix array of the text T (uint8) built on the device (tpz_sa_build)."""
+    L = lib()
+    L.tpz_sa_build.argtypes = [_VP, _I64, _VP, _VP]
+    T = np.ascontiguousarray(T, dtype=np.uint8)
+    SA = np.empty(max(len(T), 1), np.int64)
+    check(L.tpz_sa_build(_p(T), len(T), _p(SA), None))
+    return SA[:len(T)]
+
+
 def last_launches() -> int:
     return int(lib().tpz_sw_last_launches())
 
