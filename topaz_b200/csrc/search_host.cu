@@ -736,14 +736,15 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     DevBuf b;
     uint8_t *dq, *dscratch; int64_t *dqo, *dpb, *dcb; int32_t *dql, *dqs; int8_t *dsub;
     Cursor *dcur; Hit *dhits; QueryOut *dqout; PopRec *dtrace = nullptr;
-    int32_t *dqnext; uint32_t *dcache;
+    int32_t *dqnext, *dcprot; uint32_t *dcache;
     int rc;
     if ((rc = b.alloc(&dq, bytes + 1)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
         (rc = b.alloc(&dpb, nq + 1)) || (rc = b.alloc(&dcb, nq + 1)) || (rc = b.alloc(&dqs, nq)) ||
         (rc = b.alloc(&dsub, 625)) || (rc = b.alloc(&dcur, 2 * npos + 1)) ||
         (rc = b.alloc(&dscratch, per_q * nq)) || (rc = b.alloc(&dhits, (size_t)nq * max_cap)) ||
         (rc = b.alloc(&dqout, nq)) || (rc = b.alloc(&dqnext, 2 * npos + 1)) ||
-        (rc = b.alloc(&dcache, (size_t)kChain * (2 * npos + 1))))
+        (rc = b.alloc(&dcache, (size_t)kChain * (2 * npos + 1))) ||
+        (rc = b.alloc(&dcprot, (size_t)kChain * (2 * npos + 1))))
         return rc;
     if (o->trace_pops > 0 && (rc = b.alloc(&dtrace, (size_t)nq * o->trace_pops))) return rc;
     TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
@@ -768,7 +769,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         sa.chain = kChain;
         seed_kernel<<<(unsigned)std::min<int64_t>((npos + 127) / 128, (int64_t)nsm * 16), 128>>>(ix->d, sa);
         chain_kernel<<<(unsigned)std::min<int64_t>((2 * npos * kChain + 255) / 256, (int64_t)nsm * 64),
-                       256>>>(ix->d, sa, o->min_hit_length, dcache);
+                       256>>>(ix->d, sa, o->min_hit_length, dcache, dcprot);
     }
     WalkArgs wa;
     wa.qcat = dq; wa.qoff = dqo; wa.qlen = dql; wa.nq = (int)nq; wa.cursor_base = dcb;
@@ -777,7 +778,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     wa.max_cap = max_cap; wa.hash_size = hash_size; wa.max_cursors = max_cursors;
     wa.scratch = dscratch; wa.scratch_per_query = per_q; wa.hits = dhits; wa.qout = dqout;
     wa.qstatus = dqs; wa.trace = dtrace; wa.trace_cap = o->trace_pops;
-    wa.qnext = dqnext; wa.ccache = dcache;
+    wa.qnext = dqnext; wa.ccache = dcache; wa.cprot = dcprot;
     TPZ_CUDA(cudaEventRecord(ev[1], 0));
     walk_kernel<<<(unsigned)((nq + kWalkWarps - 1) / kWalkWarps), kWalkWarps * 32>>>(ix->d, wa);
     TPZ_CUDA(cudaGetLastError());

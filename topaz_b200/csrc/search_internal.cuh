@@ -25,6 +25,7 @@ struct Cursor {
     int16_t dir;
     uint8_t cpos, cn;    // next unused / valid entries of the cursor's element cache
     int32_t score, len;
+    int32_t prot;        // protein of the current row
 };
 
 constexpr int kWalkWarps = 4;            // queries (warps) per walk block
@@ -72,6 +73,7 @@ struct WalkArgs {
     size_t scratch_per_query;
     int32_t *qnext;               // per cursor (global cursor index)
     uint32_t *ccache;             // 32 packed chain elements per cursor
+    int32_t *cprot;               // the protein of each chain element's row
     Hit *hits;                    // nq * max_cap
     QueryOut *qout;
     const int32_t *qstatus;
@@ -83,7 +85,8 @@ __global__ void nl_block_count_kernel(const uint8_t *T, int64_t Tsize, int64_t n
 __global__ void lb_build_kernel(const uint8_t *T, int64_t Tsize, const int64_t *SA, int64_t *lb);
 __global__ void seed_kernel(DevIndex ix, SeedArgs a);
 __global__ void walk_kernel(DevIndex ix, WalkArgs a);
-__global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32_t *cache);
+__global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32_t *cache,
+                             int32_t *cprot);
 __global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t *qoff,
                                  const int32_t *qlen, const int32_t *query_of, const int32_t *off,
                                  const int64_t *row, int64_t n, const int8_t *sub, int32_t *score,

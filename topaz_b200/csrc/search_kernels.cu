@@ -200,8 +200,8 @@ __global__ void seed_kernel(DevIndex ix, SeedArgs a) {
         const uint8_t *Q = a.qcat + a.qoff[q];
         const int qlen = a.qlen[q];
         Cursor c0, c1;
-        c0.row = -1; c0.off = i; c0.dir = 1; c0.cpos = 0; c0.cn = a.chain; c0.score = 0; c0.len = -1;
-        c1.row = -1; c1.off = i; c1.dir = -1; c1.cpos = 0; c1.cn = a.chain; c1.score = 0; c1.len = -1;
+        c0.row = -1; c0.off = i; c0.dir = 1; c0.cpos = 0; c0.cn = a.chain; c0.prot = -1; c0.score = 0; c0.len = -1;
+        c1.row = -1; c1.off = i; c1.dir = -1; c1.cpos = 0; c1.cn = a.chain; c1.prot = -1; c1.score = 0; c1.len = -1;
         if (Q[i] != 'V') {                     // _bad_prefix: internal 'V' = X
             const int64_t pos = lower_bound(ix, Q + i, qlen - i);
             if (a.lb_out) a.lb_out[g] = pos;
@@ -209,12 +209,16 @@ __global__ void seed_kernel(DevIndex ix, SeedArgs a) {
                 atomicOr(&a.qstatus[q], TPZ_Q_SA_END);
             } else {
                 int sc = 0;
-                int ln = hsp_at(ix, ix.SA[pos], Q, qlen, i, a.sub, &sc);
+                const int64_t t0 = ix.SA[pos];
+                int ln = hsp_at(ix, t0, Q, qlen, i, a.sub, &sc);
                 c0.row = pos; c0.score = sc; c0.len = ln;
+                c0.prot = (int32_t)protein_of(ix, t0);
                 if (pos != 0) {
                     sc = 0;
-                    ln = hsp_at(ix, ix.SA[pos - 1], Q, qlen, i, a.sub, &sc);
+                    const int64_t t1 = ix.SA[pos - 1];
+                    ln = hsp_at(ix, t1, Q, qlen, i, a.sub, &sc);
                     c1.row = pos - 1; c1.score = sc; c1.len = ln;
+                    c1.prot = (int32_t)protein_of(ix, t1);
                 }
             }
         } else if (a.lb_out) {
@@ -289,22 +293,27 @@ __device__ __forceinline__ int elem_score(uint32_t e) { return (int)(int16_t)(e 
 __device__ __forceinline__ int elem_len(uint32_t e) { return (int)(int16_t)(e >> 16); }
 
 // The chain element of a cursor `step` rows past `row` (step >= 1): the
-// sa_hsp (src/suffix.c:47) of suffix_increment's next row, or a marker.
+// sa_hsp (src/suffix.c:47) of suffix_increment's next row, or a marker; and
+// the protein of that row (db_index, the hitlist's key), -1 with a marker.
 __device__ __forceinline__ uint32_t chain_elem(const DevIndex &ix, int64_t row, int dir, int step,
                                                const uint8_t *Q, int qlen, int off,
-                                               const int8_t *sub) {
+                                               const int8_t *sub, int32_t *prot) {
     const int64_t nr = row + (int64_t)dir * step;
+    *prot = -1;
     if (nr < 0 || nr >= 8 * ix.Tsize) return pack_elem(0, kLenEnd);
     if (nr >= ix.sa_rows) return pack_elem(0, kLenFault);
     int sc = 0;
-    const int ln = hsp_at(ix, ix.SA[nr], Q, qlen, off, sub, &sc);
+    const int64_t pos = ix.SA[nr];
+    const int ln = hsp_at(ix, pos, Q, qlen, off, sub, &sc);
+    *prot = (int32_t)protein_of(ix, pos);
     return pack_elem(sc, ln);
 }
 
 // One thread per (cursor, element): the first kChain chain elements of every
 // queued cursor, so that the walk, whose pops run one after another, finds
 // them ready.  Elements a cursor never reaches are computed and not used.
-__global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32_t *cache) {
+__global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32_t *cache,
+                             int32_t *cprot) {
     const int64_t total = 2 * a.npos * kChain;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total;
          x += (int64_t)gridDim.x * blockDim.x) {
@@ -318,8 +327,10 @@ __global__ void chain_kernel(DevIndex ix, SeedArgs a, int min_hit_length, uint32
             const int mid = (lo + hi + 1) >> 1;
             if (a.pos_base[mid] <= g) lo = mid; else hi = mid - 1;
         }
+        int32_t pr;
         cache[x] = chain_elem(ix, cu.row, cu.dir, e + 1, a.qcat + a.qoff[lo], a.qlen[lo], cu.off,
-                              a.sub);
+                              a.sub, &pr);
+        cprot[x] = pr;
     }
 }
 
@@ -377,6 +388,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
     Cursor *cur = a.cursors + cbase;
     int32_t *qnext = a.qnext + cbase;
     uint32_t *cache = a.ccache + cbase * 32;
+    int32_t *cprot = a.cprot + cbase * 32;
     HitView v = hit_view(a, q);
     const int cap = qlen > 3000 ? (int)(1.5 * a.num_hits) : a.alignments;   // hit.c:106-109
 
@@ -435,13 +447,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
         if (c < 0) break;
         need = __shfl_sync(0xFFFFFFFFu, need, 0);
         uint32_t elem = 0;
+        int32_t eprot = -1;
         if (need) {
             // all lanes: the next 32 rows of this cursor
             row = __shfl_sync(0xFFFFFFFFu, row, 0);
             off = __shfl_sync(0xFFFFFFFFu, off, 0);
             dir = __shfl_sync(0xFFFFFFFFu, dir, 0);
-            elem = chain_elem(ix, row, dir, lane + 1, Q, qlen, off, a.sub);
+            elem = chain_elem(ix, row, dir, lane + 1, Q, qlen, off, a.sub, &eprot);
             cache[(int64_t)c * 32 + lane] = elem;
+            cprot[(int64_t)c * 32 + lane] = eprot;
             __syncwarp();
         }
         int stop = 0;
@@ -451,9 +465,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
                 cc.cn = 32;
             } else {
                 elem = cache[(int64_t)c * 32 + cc.cpos];
+                eprot = cprot[(int64_t)c * 32 + cc.cpos];
                 cc.cpos++;
             }
-            const int gs = cc.score, gl = cc.len;
+            const int gs = cc.score, gl = cc.len, gprot = cc.prot;
             // suffix_increment + suffix_active
             const int ln = elem_len(elem);
             if (ln == kLenFault) {
@@ -463,6 +478,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
                 if (ln != kLenEnd) {
                     cc.row = row + dir;
                     cc.len = ln;
+                    cc.prot = eprot;
                     if (ln >= minlen) {
                         const int sc = elem_score(elem);
                         cc.score = sc;
@@ -481,7 +497,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
                 if (hsize >= cap && hmin >= gs) {
                     counted = true;            // full and the worst hit is at least as good
                 } else {
-                    const int p = (int)protein_of(ix, ix.SA[row]);
+                    const int p = gprot;      // protein_of(ix, ix.SA[row])
                     uint32_t hh = hash32((uint32_t)p) & hmask;
                     while (v.hkey[hh] != -1 && v.hkey[hh] != p) hh = (hh + 1) & hmask;
                     if (v.hkey[hh] == -1) {
