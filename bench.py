@@ -258,6 +258,7 @@ def search_bench(args, dev):
     torch.cuda.synchronize()
     stage = np.zeros(4)
     nh = [0]
+    swc = [0, 0]
     starts = list(range(0, len(q_aa), bsz))
     lock = threading.Lock()
 
@@ -274,6 +275,8 @@ def search_bench(args, dev):
             with lock:
                 stage[:] += np.array(r["stage_ms"])
                 nh[0] += len(r["protein"])
+                swc[0] += r["sw_pairs"]
+                swc[1] += r["sw_cells"]
 
     t0 = time.perf_counter()
     th = [threading.Thread(target=worker) for _ in range(args.search_workers)]
@@ -295,6 +298,8 @@ def search_bench(args, dev):
            "device_ms": {"seed": round(stage[0], 2), "walk_hitlist": round(stage[1], 2),
                          "sw_rank_select": round(stage[2], 2), "calls_wall": round(stage[3], 2)},
            "reported_hits_per_query": round(nh / len(q_aa), 2),
+           "sw_pairs_per_query": round(swc[0] / len(q_aa), 1),
+           "sw_gcells": round(swc[1] / 1e9, 2),
            "host_threads": args.search_workers,
            "setup_s": round(setup_s, 1), "index_load_s": round(load_s, 2),
            "sa_build_s": round(sa_s, 2), "sa_bytes": int(len(db.T)),

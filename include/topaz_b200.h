@@ -209,6 +209,7 @@ typedef struct {
                                 (+ ranking in report mode); [3] = host wall time of
                                 the whole call incl. copies */
     const double *bitscore, *evalue;         /* per hit, report mode only (else NULL) */
+    int64_t sw_pairs, sw_cells;              /* SW of hits: pairs, sum of qlen * slen */
 } tpz_search_result;
 
 TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,

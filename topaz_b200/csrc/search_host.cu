@@ -150,6 +150,17 @@ __global__ void pack_hits_kernel(PackArgs a) {
     }
 }
 
+// sum of qlen * slen over the SW pairs
+__global__ void pair_cells_kernel(int64_t n, const int32_t *ql, const int32_t *sl,
+                                  unsigned long long *cells) {
+    unsigned long long c = 0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        c += (unsigned long long)ql[k] * (unsigned long long)sl[k];
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(cells, c);
+}
+
 // SW results of pair k back to hit p_hit[k]; hit2pair (optional) records k
 __global__ void scatter_sw_kernel(int64_t n, const int32_t *p_hit, const int32_t *sc,
                                   const int32_t *re, const int32_t *rd, const int32_t *st,
@@ -330,6 +341,7 @@ struct ResultHolder {
     std::vector<int32_t> status, protein, gs, gl, so, raw, qend, send, sw_status;
     std::vector<int32_t> trace_off, trace_score, trace_len, trace_counted;
     std::vector<double> bits, evalue;
+    int64_t sw_pairs = 0, sw_cells = 0;
 };
 
 // Ranking tables of report mode.  The bitscore of a raw score does not
@@ -833,6 +845,17 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         if (cudaMemcpy(poff.data(), dpoff, 8 * (nq + 1), cudaMemcpyDeviceToHost) != cudaSuccess)
             return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch pairs"));
         const int64_t npairs = poff[nq];
+        R->sw_pairs = npairs;
+        if (npairs > 0) {
+            unsigned long long *dcells;
+            if ((rc = b.alloc(&dcells, 1))) return bail(rc);
+            TPZ_CUDA(cudaMemset(dcells, 0, 8));
+            pair_cells_kernel<<<(unsigned)std::min<int64_t>((npairs + 255) / 256, 2048), 256>>>(
+                npairs, pq_len, ps_len, dcells);
+            unsigned long long cells = 0;
+            TPZ_CUDA(cudaMemcpy(&cells, dcells, 8, cudaMemcpyDeviceToHost));
+            R->sw_cells = (int64_t)cells;
+        }
         if (npairs > 0) {
             // the pairs of a query share its profile; report mode ranks on
             // scores alone (end coordinates come later, for the reported hits)
@@ -909,6 +932,8 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     r.stage_ms[1] = t12;
     r.stage_ms[2] = t23;
     r.stage_ms[3] = (tw1.tv_sec - tw0.tv_sec) * 1e3 + (tw1.tv_usec - tw0.tv_usec) / 1e3;
+    r.sw_pairs = R->sw_pairs;
+    r.sw_cells = R->sw_cells;
     *out = &R->r;
     return TPZ_OK;
 }

@@ -140,14 +140,18 @@ __device__ __forceinline__ uint32_t letter_pair(const Args &a, const int8_t *sA,
 }
 
 // One task: pairs pA and pB (pB < 0: none) in the halves of the int16x2
-// lanes.  lanes = 16 (u8 pass) or 8 (i16 pass); u8 results that saturate go
-// to rerun[atomicAdd(rerun_count)].  BUILD = false: profA/profB already hold
-// the query profiles (both pairs then share one query).
-template <int R, bool MULTI, bool BUILD = true>
+// lanes.  The pass (16 SSW lanes = u8, 8 = i16) and the list that saturated
+// u8 results go to come from `a` (QM = false) or, for the query-major
+// kernel, from qm_lanes / qm_rerun / qm_rerun_count; QM = true also means
+// that profA/profB already hold the query profile (both pairs share it).
+template <int R, bool MULTI, bool QM = false>
 __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
                                          uint32_t *profA, uint32_t *profB, uint16_t *ring,
-                                         int stripes, uint32_t *bnd, int lanes, int32_t *rerun,
-                                         int32_t *rerun_count) {
+                                         int stripes, uint32_t *bnd, int qm_lanes = 0,
+                                         int32_t *qm_rerun = nullptr,
+                                         int32_t *qm_rerun_count = nullptr) {
+    constexpr bool BUILD = !QM;
+#define TPZ_LANES (QM ? qm_lanes : a.ssw_lanes)
     constexpr int W = words_for(R);
     const int lane = threadIdx.x & 31;
 
@@ -160,8 +164,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     const int8_t *qB = pB >= 0 ? a.q + a.qoff[pB] : qA;
     const int8_t *sB = pB >= 0 ? a.s + a.soff[pB] : sA;
     const int N = max(slA, slB);
-    const int segA = max(1, (qlA + lanes - 1) / lanes);
-    const int segB = max(1, (qlB + lanes - 1) / lanes);
+    const int segA = max(1, (qlA + TPZ_LANES - 1) / TPZ_LANES);
+    const int segB = max(1, (qlB + TPZ_LANES - 1) / TPZ_LANES);
     const uint32_t NGO = pack2(-a.gap_open, -a.gap_open);
     const uint32_t NGE = pack2(-a.gap_extend, -a.gap_extend);
     const uint32_t NEGINF = 0x80008000u;
@@ -268,7 +272,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
                 wm = __vimax_s16x2_relu(wm, __shfl_xor_sync(0xFFFFFFFFu, wm, o));
-            if (lanes == 16) {
+            if (TPZ_LANES == 16) {
                 // u8 pass: a pair whose maximum reached 255 - bias is decided
                 // (the i16 pass reruns it), so it needs no more row searches,
                 // and a task whose pairs are both decided stops here
@@ -391,11 +395,12 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             const int v = (int)(key >> 40);
             const int col = key ? 0xFFFFFF - (int)((key >> 16) & 0xFFFFFF) : -1;
             const int row = key ? 0xFFFF - (int)(key & 0xFFFF) : 0;
-            if (lanes == 16 && v + a.bias >= 255) {
+            if (TPZ_LANES == 16 && v + a.bias >= 255) {
                 // u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
-                const int slot = atomicAdd(rerun_count, 1);
-                rerun[slot] = p;
-            } else if (lanes == 8 && a.exact_list && v >= a.exact_threshold) {
+                int32_t *rr = QM ? qm_rerun : a.rerun;
+                const int slot = atomicAdd(QM ? qm_rerun_count : a.rerun_count, 1);
+                rr[slot] = p;
+            } else if (TPZ_LANES == 8 && a.exact_list && v >= a.exact_threshold) {
                 // near the i16 limit: 16-bit lanes may wrap, redo in 32 bits
                 const int slot = atomicAdd(a.exact_count, 1);
                 a.exact_list[slot] = p;
@@ -408,6 +413,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
         }
     }
 }
+
+#undef TPZ_LANES
 
 template <int R>
 __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args a, int bin,
@@ -438,13 +445,11 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
         if constexpr (R == kMaxR) {
             if (stripes > 1) {
                 run_task<R, true>(a, pA, pB, smat, profA, profB, ring, stripes,
-                                  a.bnd + (size_t)blockIdx.x * a.bnd_words, a.ssw_lanes, a.rerun,
-                                  a.rerun_count);
+                                  a.bnd + (size_t)blockIdx.x * a.bnd_words);
                 continue;
             }
         }
-        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr, a.ssw_lanes, a.rerun,
-                           a.rerun_count);
+        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr);
     }
 }
 
@@ -472,12 +477,12 @@ __global__ void __launch_bounds__(32) sw_one_kernel(const __grid_constant__ Args
     b.qoff = &s_off; b.soff = &s_off; b.qlen = &s_ql; b.slen = &s_sl;
     b.rerun_count = &s_rr[0]; b.rerun = &s_rr[1];
     b.ssw_lanes = 16;
-    run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr, 16, b.rerun, b.rerun_count);
+    run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr);
     __syncwarp();
     if (s_rr[0]) {
         // the u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
         b.ssw_lanes = 8;
-        run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr, 8, b.rerun, b.rerun_count);
+        run_task<R, false>(b, 0, -1, smat, profA, profB, ring, 1, nullptr);
     }
 }
 
@@ -596,8 +601,8 @@ __global__ void __launch_bounds__(kQmWarps * 32) sw_query_kernel(const __grid_co
             if (2 * t >= n) break;
             const int pA = (int)(uint32_t)keys[2 * t];
             const int pB = 2 * t + 1 < n ? (int)(uint32_t)keys[2 * t + 1] : -1;
-            run_task<R, false, false>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 16, sat,
-                                      &s_nsat);
+            run_task<R, false, true>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 16, sat,
+                                     &s_nsat);
         }
         __syncthreads();
         if (threadIdx.x == 0) s_next = 0;
@@ -611,8 +616,8 @@ __global__ void __launch_bounds__(kQmWarps * 32) sw_query_kernel(const __grid_co
             if (2 * t >= ns) break;
             const int pA = sat[2 * t];
             const int pB = 2 * t + 1 < ns ? sat[2 * t + 1] : -1;
-            run_task<R, false, false>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 8, nullptr,
-                                      nullptr);
+            run_task<R, false, true>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 8, nullptr,
+                                     nullptr);
         }
     }
 }

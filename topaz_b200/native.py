@@ -164,7 +164,8 @@ class _SearchResult(ctypes.Structure):
                 ("trace_off", _P32), ("trace_score", _P32), ("trace_len", _P32),
                 ("trace_counted", _P32), ("stage_ms", ctypes.c_double * 4),
                 ("bitscore", ctypes.POINTER(ctypes.c_double)),
-                ("evalue", ctypes.POINTER(ctypes.c_double))]
+                ("evalue", ctypes.POINTER(ctypes.c_double)),
+                ("sw_pairs", ctypes.c_int64), ("sw_cells", ctypes.c_int64)]
 
 
 def _search_sigs(L):
@@ -286,6 +287,7 @@ class Index:
                       "qend", "send", "sw_status"):
                 out[k] = arr(getattr(r, k), nh)
             out["stage_ms"] = list(r.stage_ms)
+            out["sw_pairs"], out["sw_cells"] = int(r.sw_pairs), int(r.sw_cells)
             if report is not None:
                 out["bitscore"] = arr(r.bitscore, nh)
                 out["evalue"] = arr(r.evalue, nh)
