@@ -178,7 +178,7 @@ def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.
     qres, qlens = synth.search_queries_arrays(res, lens, 4000, 4000, seed=args.seed + 21,
                                               lo=30, hi=3000)
     qoff = np.cumsum(qlens) - qlens
-    pool = [native.prepare_query(qres[o:o + n].tobytes()) for o, n in zip(qoff, qlens)]
+    pool = native.prepare_queries([qres[o:o + n].tobytes() for o, n in zip(qoff, qlens)])
     rng = np.random.Generator(np.random.PCG64(args.seed + 22))
     workers, max_batch = 3, 2000
     srv = serve.SearchServer(ix, mat, workers=workers, max_batch=max_batch,
@@ -245,7 +245,7 @@ def search_bench(args, dev):
     bsz = args.search_batch
     # warm-up: one full-size batch per worker thread, so that the device
     # memory pool of every thread has grown to a batch before the timing
-    warm = [native.prepare_query(q) for q in q_aa[:bsz]]
+    warm = native.prepare_queries(q_aa[:bsz])
 
     def warm_one():
         ix.search(warm, mat, report=report)
@@ -270,7 +270,7 @@ def search_bench(args, dev):
                 if not starts:
                     return
                 b = starts.pop(0)
-            qs = [native.prepare_query(q) for q in q_aa[b:b + bsz]]
+            qs = native.prepare_queries(q_aa[b:b + bsz])
             r = ix.search(qs, mat, report=report)
             with lock:
                 stage[:] += np.array(r["stage_ms"])
@@ -292,7 +292,8 @@ def search_bench(args, dev):
               "mid-size config), batches of %d" % (args.search_proteins, args.search_queries, bsz))
     out = {"workload": wl, "queries": len(q_aa), "queries_per_s": round(len(q_aa) / wall, 1),
            "wall_s": round(wall, 3),
-           "api": "tpz_search_batch report mode (host buffers; SEG + alphabet on the host, "
+           "api": "tpz_search_batch report mode (host buffers; SEG + alphabet on the host by "
+                  "tpz_prepare_queries, "
                   "ranking and -H/-E cut on the device, all inside the timed region; "
                   "batches from %d host threads)" % args.search_workers,
            "device_ms": {"seed": round(stage[0], 2), "walk_hitlist": round(stage[1], 2),

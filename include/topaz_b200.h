@@ -217,6 +217,15 @@ TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_
                              tpz_search_result **out);
 TPZ_API void tpz_search_result_free(tpz_search_result *r);
 
+/* Query ingest of a batch, in place (run_seg + seq_2internal,
+ * src/engine.c:250-277): query i = cat[off[i] .. off[i]+len[i]) holds
+ * upper-case residues (as the FASTA reader gives them); with seg != 0 SEG
+ * hard-masks it (seg_wrapper.c:15-49), then every residue becomes its
+ * internal-alphabet letter, the form tpz_search_batch takes.  Runs on
+ * nthreads host threads. */
+TPZ_API int tpz_prepare_queries(char *cat, const int64_t *off, const int32_t *len, int64_t n,
+                                int seg, int nthreads);
+
 /* Suffix array of the .psq bytes T[0, n) on the device, for `topaz index`
  * (serif_index / create_index, src/index.c:24-93, build it on the host):
  * SA[0, n) (host) receives the suffixes in byte-lexicographic order, a

@@ -58,6 +58,23 @@ def test_seg_matches_golden():
         assert buf.raw[:len(s)] == masked[off[i]:off[i + 1]], i
 
 
+def test_prepare_queries_batch_matches_golden_seg():
+    """tpz_prepare_queries (SEG + internal alphabet over host threads) on the
+    golden SEG inputs equals SEG then the alphabet query by query."""
+    from topaz_b200 import alphabet as ab, native
+    g = np.load(os.path.join(HERE, "golden", "seg_golden.npz"))
+    seqs, masked = g["seqs"].tobytes(), g["masked"].tobytes()
+    off = g["off"]
+    qs = [seqs[off[i]:off[i + 1]] for i in range(len(off) - 1)]
+    want = [ab.aa_to_internal(np.frombuffer(masked[off[i]:off[i + 1]], np.uint8)).tobytes()
+            for i in range(len(off) - 1)]
+    for threads in (1, 3, 16):
+        assert native.prepare_queries(qs, threads=threads) == want
+    nos = native.prepare_queries(qs, seg=False, threads=2)
+    assert nos == [ab.aa_to_internal(np.frombuffer(q, np.uint8)).tobytes() for q in qs]
+    assert native.prepare_queries([]) == []
+
+
 @needs_ref
 def test_seg_matches_live_reference():
     L, R = host(), oracle.libref()

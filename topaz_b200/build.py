@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["tpz_common.cu", "sw_kernel.cu", "search_kernels.cu", "search_host.cu", "sa_build.cu"]
 HOSTDIR = os.path.join(HERE, "host")
 HOST_SOURCES = ["tpzh_fasta.c", "tpzh_seg.c", "tpzh_sais.c", "tpzh_index.c", "tpzh_stats.c",
-                "tpzh_search.c", "tpzh_main.c"]
+                "tpzh_search.c", "tpzh_main.c", "tpzh_prepare.c"]
 CLI = os.path.join(LIBDIR, "topaz")
 CC = os.environ.get("CC", "gcc")
 # plain IEEE double arithmetic in the host code (no fast-math, no FMA
@@ -77,7 +77,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             sys.stderr.write("nvcc failed on %s\n" % src)
     if failed:
         raise RuntimeError("building libtopaz_b200.so failed")
-    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xlinker", "-Bsymbolic", "-lm"]
+    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xlinker", "-Bsymbolic", "-lm", "-lpthread"]
     subprocess.check_call(link)
     cli = [CC, "-O2", "-o", CLI, os.path.join(HOSTDIR, "tpzh_cli.c"), "-I", HOSTDIR, "-L", LIBDIR,
            "-ltopaz_b200", "-Wl,-rpath,$ORIGIN", "-lm"]

@@ -188,8 +188,6 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
             const int rc = tpzh_fasta_next(&f, &r);
             if (rc < 0) exit(EXIT_FAILURE);
             if (rc == 0) { done = 1; break; }
-            if (o->seg_enabled) tpzh_seg_mask(r.seq, r.seq_len);
-            for (int i = 0; i < r.seq_len; ++i) r.seq[i] = tpzh_aa2internal(r.seq[i]);
             qs[nq].id = r.id; qs[nq].id_len = r.id_len;
             qs[nq].seq = r.seq; qs[nq].len = r.seq_len;
             nq++;
@@ -201,6 +199,10 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
         for (int64_t i = 0; i < nq; ++i) { qoff[i] = total; qlen[i] = qs[i].len; total += qs[i].len; }
         char *cat = malloc(total + 1);
         for (int64_t i = 0; i < nq; ++i) memcpy(cat + qoff[i], qs[i].seq, qs[i].len);
+        /* run_seg + seq_2internal for the whole batch over host threads */
+        const long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+        tpz_prepare_queries(cat, qoff, qlen, nq, o->seg_enabled, ncpu > 0 ? (int)ncpu : 1);
+        for (int64_t i = 0; i < nq; ++i) memcpy(qs[i].seq, cat + qoff[i], qs[i].len);
         tpz_search_result *res = NULL;
         if (tpz_search_batch(ix, cat, qoff, qlen, nq, &so, &res) != 0) {
             fprintf(stderr, "Error: %s\n", tpz_last_error());

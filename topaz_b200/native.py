@@ -319,6 +319,19 @@ def seg_mask(residues: bytes) -> bytes:
     return buf.raw[:len(residues)]
 
 
+def prepare_queries(queries, seg: bool = True, threads: int = 0):
+    """prepare_query for a list of queries in one library call
+    (tpz_prepare_queries), on `threads` host threads (0: all cores)."""
+    L = lib()
+    L.tpz_prepare_queries.argtypes = [_VP, _VP, _VP, _I64, ctypes.c_int, ctypes.c_int]
+    cat, off, lens = _concat(queries)
+    cat = cat.copy()
+    check(L.tpz_prepare_queries(_p(cat), _p(off), _p(lens), len(queries), 1 if seg else 0,
+                                threads or (os.cpu_count() or 1)))
+    b = cat.tobytes()
+    return [b[o:o + n] for o, n in zip(off.tolist(), lens.tolist())]
+
+
 def prepare_query(residues: bytes, seg: bool = True) -> bytes:
     """A FASTA query as the search kernels take it: SEG (unless disabled),
     then the internal alphabet (run_seg + seq_2internal)."""
