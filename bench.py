@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--search-workers", type=int, default=2,
                     help="host threads issuing search batches concurrently")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop section")
+    ap.add_argument("--search-large", action="store_true",
+                    help="add a full search on a large DB (default and --fast)")
+    ap.add_argument("--large-proteins", type=int, default=10_000_000)
+    ap.add_argument("--large-queries", type=int, default=20_000)
     ap.add_argument("--search-proteins", type=int, default=1_000_000,
                     help="DB size of the full-search section (proteins)")
     ap.add_argument("--search-queries", type=int, default=10_000,
@@ -209,6 +213,68 @@ def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.
     srv.close()
     return {"workload": SERVE_WORKLOAD % (workers, max_batch), "capacity_qps": round(capacity_qps, 1),
             "loads": rows, "api": "topaz_b200.serve.SearchServer over tpz_search_batch report mode"}
+
+
+def large_bench(args, dev):
+    """Full search on a larger DB than the mid-size config: index built on the
+    device, default and --fast sensitivity, report mode, 2 host threads."""
+    import torch
+
+    from topaz_b200 import dbformat, native, synth
+    t0 = time.perf_counter()
+    res, lens = synth.protein_db_arrays(args.large_proteins, seed=args.seed + 31)
+    db = dbformat.build_from_arrays(res, lens)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    db.SA = native.sa_build(db.T)
+    sa_s = time.perf_counter() - t0
+    torch.cuda.empty_cache()
+    qres, qlens = synth.search_queries_arrays(res, lens, args.large_queries // 2,
+                                              args.large_queries - args.large_queries // 2,
+                                              seed=args.seed + 32)
+    qoff = np.cumsum(qlens) - qlens
+    qs = native.prepare_queries([qres[o:o + n].tobytes() for o, n in zip(qoff, qlens)])
+    del res
+    t0 = time.perf_counter()
+    ix = native.Index(db)
+    load_s = time.perf_counter() - t0
+    mat = synth.matrix("BLOSUM62")
+    report = {"max_evalue": 1e-3}
+    bsz = args.search_batch
+    out = {"workload": "full search, large: %d-protein synthetic DB (%.2f G residues, log-normal "
+                       "lengths median 300, 50-2000), %d queries of 50-1500 residues (half mutated, "
+                       "half random), SEG on, BLOSUM62 11/1, -H 100 -E 1e-3, batches of %d from 2 "
+                       "host threads" % (args.large_proteins, len(db.T) / 1e9, len(qs), bsz),
+           "db_bytes": int(len(db.T)), "generate_s": round(gen_s, 1), "sa_build_s": round(sa_s, 2),
+           "index_load_s": round(load_s, 2), "index_device_gb": round(ix.device_bytes / 1e9, 2)}
+    for mode, seeds, aligns in (("default", 300000, 5000), ("fast", 100000, 1500)):
+        ix.search(qs[:bsz], mat, report=report, seeds=seeds, alignments=aligns)   # warm-up
+        starts = list(range(0, len(qs), bsz))
+        lock = threading.Lock()
+        nh = [0]
+
+        def worker():
+            while True:
+                with lock:
+                    if not starts:
+                        return
+                    b = starts.pop(0)
+                r = ix.search(qs[b:b + bsz], mat, report=report, seeds=seeds, alignments=aligns)
+                with lock:
+                    nh[0] += len(r["protein"])
+
+        t0 = time.perf_counter()
+        th = [threading.Thread(target=worker) for _ in range(2)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+        out[mode] = {"queries_per_s": round(len(qs) / wall, 1), "wall_s": round(wall, 2),
+                     "seeds": seeds, "alignments": aligns,
+                     "reported_hits_per_query": round(nh[0] / len(qs), 2)}
+    ix.close()
+    return out
 
 
 def search_bench(args, dev):
@@ -512,10 +578,14 @@ def native_arm(args, rank, local_rank, world):
 
     line = None
     search = None
+    large = None
     if rank == 0 and world == 1 and not args.no_search:
         del t, pin, outs
         torch.cuda.empty_cache()
         search = search_bench(args, dev)
+    if rank == 0 and world == 1 and args.search_large:
+        torch.cuda.empty_cache()
+        large = large_bench(args, dev)
     if rank == 0:
         cpu = None if args.no_cpu_baseline else cpu_baseline_sw(ps, mat)
         traffic_per_cell = read_traffic()
@@ -543,6 +613,8 @@ def native_arm(args, rank, local_rank, world):
             "step_ms": [round(x, 3) for x in step_ms],
             "search": search,
         }
+        if large is not None:
+            line["search_large"] = large
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
