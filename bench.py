@@ -215,6 +215,28 @@ def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.
             "loads": rows, "api": "topaz_b200.serve.SearchServer over tpz_search_batch report mode"}
 
 
+def seed_roofline(positions, ms, tsize):
+    """Seed lookup against HBM: algorithmic bytes per searched position =
+    ceil(log2(Tsize+1)) x (8 B SA entry + 32 B text sector) -- the binary
+    search of sa_search; the kernel's prefix table skips most of those steps,
+    so the figure is the work it stands in for, not its own traffic."""
+    peak = measured_hbm_gbs()
+    steps = int(np.ceil(np.log2(tsize + 1)))
+    gb = positions * steps * 40 / 1e9
+    ach = gb / (ms / 1e3) if ms > 0 else None
+    return {"positions": int(positions), "device_ms": round(ms, 2),
+            "algorithmic_gb": round(gb, 2), "achieved_gbs": round(ach, 1) if ach else None,
+            "peak_gbs": peak, "frac": round(ach / peak, 3) if ach and peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy)"}
+
+
+def measured_hbm_gbs():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
 def large_bench(args, dev):
     """Full search on a larger DB than the mid-size config: index built on the
     device, default and --fast sensitivity, report mode, 2 host threads."""
@@ -324,7 +346,7 @@ def search_bench(args, dev):
     torch.cuda.synchronize()
     stage = np.zeros(4)
     nh = [0]
-    swc = [0, 0]
+    swc = [0, 0, 0.0, 0.0, 0]
     starts = list(range(0, len(q_aa), bsz))
     lock = threading.Lock()
 
@@ -343,6 +365,9 @@ def search_bench(args, dev):
                 nh[0] += len(r["protein"])
                 swc[0] += r["sw_pairs"]
                 swc[1] += r["sw_cells"]
+                swc[2] += r["seed_ms"]
+                swc[3] += r["chain_ms"]
+                swc[4] += r["positions"]
 
     t0 = time.perf_counter()
     th = [threading.Thread(target=worker) for _ in range(args.search_workers)]
@@ -367,6 +392,7 @@ def search_bench(args, dev):
            "reported_hits_per_query": round(nh / len(q_aa), 2),
            "sw_pairs_per_query": round(swc[0] / len(q_aa), 1),
            "sw_gcells": round(swc[1] / 1e9, 2),
+           "seed_lookup": seed_roofline(swc[4], swc[2], len(db.T)),
            "host_threads": args.search_workers,
            "setup_s": round(setup_s, 1), "index_load_s": round(load_s, 2),
            "sa_build_s": round(sa_s, 2), "sa_bytes": int(len(db.T)),

@@ -210,6 +210,8 @@ typedef struct {
                                 the whole call incl. copies */
     const double *bitscore, *evalue;         /* per hit, report mode only (else NULL) */
     int64_t sw_pairs, sw_cells;              /* SW of hits: pairs, sum of qlen * slen */
+    double seed_ms, chain_ms;                /* stage_ms[0] split: seed lookup, cursor chains */
+    int64_t positions;                       /* query positions searched */
 } tpz_search_result;
 
 TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,

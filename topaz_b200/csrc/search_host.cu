@@ -770,9 +770,9 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     const int nsm = tpz::sm_count();
     struct timeval tw0, tw1;
     gettimeofday(&tw0, nullptr);
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[5];          // start, walk start, walk end, SW end, seeds done
     for (auto &e : ev) TPZ_CUDA(cudaEventCreate(&e));
-    struct EvFree { cudaEvent_t *e; ~EvFree() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); } } evfree{ev};
+    struct EvFree { cudaEvent_t *e; ~EvFree() { for (int i = 0; i < 5; ++i) cudaEventDestroy(e[i]); } } evfree{ev};
     TPZ_CUDA(cudaEventRecord(ev[0], 0));
     if (npos > 0) {
         SeedArgs sa;
@@ -780,6 +780,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         sa.npos = npos; sa.sub = dsub; sa.cursors = dcur; sa.lb_out = nullptr; sa.qstatus = dqs;
         sa.chain = kChain;
         seed_kernel<<<(unsigned)std::min<int64_t>((npos + 127) / 128, (int64_t)nsm * 16), 128>>>(ix->d, sa);
+        TPZ_CUDA(cudaEventRecord(ev[4], 0));
         chain_kernel<<<(unsigned)std::min<int64_t>((2 * npos * kChain + 255) / 256, (int64_t)nsm * 64),
                        256>>>(ix->d, sa, o->min_hit_length, dcache, dcprot);
     }
@@ -925,6 +926,11 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     TPZ_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
     float t01 = 0, t12 = 0, t23 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    float t04 = 0;
+    if (npos > 0) cudaEventElapsedTime(&t04, ev[0], ev[4]);
+    r.seed_ms = t04;
+    r.chain_ms = npos > 0 ? t01 - t04 : 0;
+    r.positions = npos;
     cudaEventElapsedTime(&t12, ev[1], ev[2]);
     if (nh > 0) cudaEventElapsedTime(&t23, ev[2], ev[3]);
     gettimeofday(&tw1, nullptr);

@@ -165,7 +165,9 @@ class _SearchResult(ctypes.Structure):
                 ("trace_counted", _P32), ("stage_ms", ctypes.c_double * 4),
                 ("bitscore", ctypes.POINTER(ctypes.c_double)),
                 ("evalue", ctypes.POINTER(ctypes.c_double)),
-                ("sw_pairs", ctypes.c_int64), ("sw_cells", ctypes.c_int64)]
+                ("sw_pairs", ctypes.c_int64), ("sw_cells", ctypes.c_int64),
+                ("seed_ms", ctypes.c_double), ("chain_ms", ctypes.c_double),
+                ("positions", ctypes.c_int64)]
 
 
 def _search_sigs(L):
@@ -288,6 +290,8 @@ class Index:
                 out[k] = arr(getattr(r, k), nh)
             out["stage_ms"] = list(r.stage_ms)
             out["sw_pairs"], out["sw_cells"] = int(r.sw_pairs), int(r.sw_cells)
+            out["seed_ms"], out["chain_ms"] = float(r.seed_ms), float(r.chain_ms)
+            out["positions"] = int(r.positions)
             if report is not None:
                 out["bitscore"] = arr(r.bitscore, nh)
                 out["evalue"] = arr(r.evalue, nh)
