@@ -347,6 +347,7 @@ def search_bench(args, dev):
     stage = np.zeros(4)
     nh = [0]
     swc = [0, 0, 0.0, 0.0, 0]
+    pops = []
     starts = list(range(0, len(q_aa), bsz))
     lock = threading.Lock()
 
@@ -368,6 +369,7 @@ def search_bench(args, dev):
                 swc[2] += r["seed_ms"]
                 swc[3] += r["chain_ms"]
                 swc[4] += r["positions"]
+                pops.extend(r["npops"].tolist())
 
     t0 = time.perf_counter()
     th = [threading.Thread(target=worker) for _ in range(args.search_workers)]
@@ -393,6 +395,9 @@ def search_bench(args, dev):
            "sw_pairs_per_query": round(swc[0] / len(q_aa), 1),
            "sw_gcells": round(swc[1] / 1e9, 2),
            "seed_lookup": seed_roofline(swc[4], swc[2], len(db.T)),
+           "pops_per_query": {"mean": round(float(np.mean(pops)), 1),
+                              "p50": int(np.percentile(pops, 50)), "p99": int(np.percentile(pops, 99)),
+                              "max": int(np.max(pops))},
            "host_threads": args.search_workers,
            "setup_s": round(setup_s, 1), "index_load_s": round(load_s, 2),
            "sa_build_s": round(sa_s, 2), "sa_bytes": int(len(db.T)),
