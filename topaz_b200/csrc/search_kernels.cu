@@ -99,22 +99,58 @@ __device__ int hsp_at(const DevIndex &ix, int64_t idx, const uint8_t *Q, int qle
     int64_t mr = ix.Tsize - idx;
     if (mr > qlen - off) mr = qlen - off;
     if (mr > 128) mr = 128;
+    // bytes in chunks of 8: the loads of a chunk go out together (only
+    // bytes inside the window are read), then the running sum walks them
+    // in order and stops at the first '\n' exactly as the byte loop does
+    constexpr int kC = 8;
     int run = 0, best_r = 0, arg_r = 0;
-    for (int i = 0; i < (int)mr; ++i) {
-        const uint8_t c = t[i];
-        if (c == '\n') break;
-        run += sub[(c - 'A') * 25 + (q[i] - 'A')];
-        if (run >= best_r) { best_r = run; arg_r = i; }
+    for (int i = 0; i < (int)mr; i += kC) {
+        uint8_t c[kC], d[kC];
+#pragma unroll
+        for (int k = 0; k < kC; ++k) {
+            const bool in = i + k < (int)mr;
+            c[k] = in ? t[i + k] : (uint8_t)'\n';
+            d[k] = in ? q[i + k] : (uint8_t)'A';
+        }
+        bool stop = false;
+#pragma unroll
+        for (int k = 0; k < kC; ++k) {
+            if (!stop) {
+                if (c[k] == '\n') {
+                    stop = true;
+                } else {
+                    run += sub[(c[k] - 'A') * 25 + (d[k] - 'A')];
+                    if (run >= best_r) { best_r = run; arg_r = i + k; }
+                }
+            }
+        }
+        if (stop) break;
     }
     int64_t ml = idx < off ? idx : off;
     if (ml > 128) ml = 128;
     int best_l = 0, arg_l = 0;
     run = 0;
-    for (int i = 1; i < (int)ml; ++i) {
-        const uint8_t c = t[-i];
-        if (c == '\n') break;
-        run += sub[(c - 'A') * 25 + (q[-i] - 'A')];
-        if (run >= best_l) { best_l = run; arg_l = i; }
+    for (int i = 1; i < (int)ml; i += kC) {
+        uint8_t c[kC], d[kC];
+#pragma unroll
+        for (int k = 0; k < kC; ++k) {
+            const bool in = i + k < (int)ml;
+            c[k] = in ? t[-(i + k)] : (uint8_t)'\n';
+            d[k] = in ? q[-(i + k)] : (uint8_t)'A';
+        }
+        bool stop = false;
+#pragma unroll
+        for (int k = 0; k < kC; ++k) {
+            if (!stop) {
+                if (c[k] == '\n') {
+                    stop = true;
+                } else {
+                    run += sub[(c[k] - 'A') * 25 + (d[k] - 'A')];
+                    if (run >= best_l) { best_l = run; arg_l = i + k; }
+                }
+            }
+        }
+        if (stop) break;
     }
     *score = best_l + best_r;
     return arg_l + arg_r;
