@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--pairs", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--search-workers", type=int, default=2,
+    ap.add_argument("--search-workers", type=int, default=3,
                     help="host threads issuing search batches concurrently")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop section")
     ap.add_argument("--search-large", action="store_true",

@@ -29,7 +29,7 @@ struct Cursor {
 };
 
 constexpr int kWalkWarps = 4;            // queries (warps) per walk block
-constexpr int kChain = 32;               // chain elements cached per cursor
+constexpr int kChain = 64;               // chain elements cached per cursor
 
 struct Hit {
     int32_t protein, gapless_score, gapless_length, suffix_offset;

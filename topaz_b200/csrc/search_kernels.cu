@@ -423,8 +423,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
     const int ncur = (int)(a.cursor_base[q + 1] - cbase);
     Cursor *cur = a.cursors + cbase;
     int32_t *qnext = a.qnext + cbase;
-    uint32_t *cache = a.ccache + cbase * 32;
-    int32_t *cprot = a.cprot + cbase * 32;
+    uint32_t *cache = a.ccache + cbase * kChain;
+    int32_t *cprot = a.cprot + cbase * kChain;
     HitView v = hit_view(a, q);
     const int cap = qlen > 3000 ? (int)(1.5 * a.num_hits) : a.alignments;   // hit.c:106-109
 
@@ -490,8 +490,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
             off = __shfl_sync(0xFFFFFFFFu, off, 0);
             dir = __shfl_sync(0xFFFFFFFFu, dir, 0);
             elem = chain_elem(ix, row, dir, lane + 1, Q, qlen, off, a.sub, &eprot);
-            cache[(int64_t)c * 32 + lane] = elem;
-            cprot[(int64_t)c * 32 + lane] = eprot;
+            cache[(int64_t)c * kChain + lane] = elem;
+            cprot[(int64_t)c * kChain + lane] = eprot;
             __syncwarp();
         }
         int stop = 0;
@@ -500,8 +500,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
                 cc.cpos = 1;
                 cc.cn = 32;
             } else {
-                elem = cache[(int64_t)c * 32 + cc.cpos];
-                eprot = cprot[(int64_t)c * 32 + cc.cpos];
+                elem = cache[(int64_t)c * kChain + cc.cpos];
+                eprot = cprot[(int64_t)c * kChain + cc.cpos];
                 cc.cpos++;
             }
             const int gs = cc.score, gl = cc.len, gprot = cc.prot;
