@@ -38,7 +38,7 @@ def query_device_bytes(qlen: int, num_hits: int = 100, alignments: int = 5000,
     hash_size = 16
     while hash_size < 2 * (cap + 1):
         hash_size <<= 1
-    per_pos = 2 * (24 + 4 + 4 * 32) + 8
+    per_pos = 2 * (32 + 4 + 8 * 64) + 8          # cursor, queue link, 64 chain elements + proteins
     hitlist = 7 * 4 * (cap + 1) + 2 * 4 * 4352 + 8 * 68 + 2 * 4 * hash_size
     hits = cap * (16 + 4 * 24)
     return npos * per_pos + hitlist + hits + qlen + 256
