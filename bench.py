@@ -503,7 +503,7 @@ def native_arm(args, rank, local_rank, world):
     import torch
     import torch.distributed as dist
 
-    from topaz_b200 import native, synth
+    from topaz_b200 import native, replicas, synth
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -561,10 +561,7 @@ def native_arm(args, rank, local_rank, world):
     assert (status == native.TPZ_SW_OK).all(), "pairs not aligned: %s" % np.unique(status)
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     total_ms = sum(step_ms)
-    tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    max_ms = float(tt.item())
+    max_ms = replicas.max_over_ranks(total_ms, world, dev)
     value = world * cells * args.steps / (max_ms / 1e3) / 1e9
     achieved = cells / (total_ms / args.steps / 1e3) / 1e9
 
@@ -595,11 +592,9 @@ def native_arm(args, rank, local_rank, world):
         e2e_step()
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        barrier()
-    e2e_val = world * cells * args.steps / float(te.item()) / 1e9
+    e2e_max_s = replicas.max_over_ranks(e2e_s, world, dev)
+    barrier()
+    e2e_val = world * cells * args.steps / e2e_max_s / 1e9
     clk = clocks.stop()         # the samples cover the device-timed and the e2e steps
     h2d = sum(v.numel() * v.element_size() for v in pin.values())
     d2h = sum(v.numel() * v.element_size() for v in outs.values())
