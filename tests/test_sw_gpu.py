@@ -103,6 +103,29 @@ def test_sw_full_size_sample_and_order_independence(cuda):
     assert (got_r[:, ::-1] == got).all()
 
 
+def test_sw_host_large_batch_matches_device(cuda):
+    # the host entry point on 160 MB of residues equals the device call on
+    # the same pairs, in any pair order, and on pairs that share a subject
+    ps = synth.sw_pairs(200_000, seed=8)
+    assert len(ps.q) + len(ps.s) > 64 << 20
+    mat = synth.matrix("BLOSUM62")
+    dev = _run_dev(cuda, ps, mat)
+    host = np.stack(native.sw_batch_host(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat))
+    assert (host == dev).all()
+    perm = np.random.default_rng(2).permutation(ps.n)
+    hp = np.stack(native.sw_batch_host(ps.q, ps.qoff[perm], ps.qlen[perm], ps.s, ps.soff[perm],
+                                       ps.slen[perm], mat))
+    assert (hp == dev[:, perm]).all()
+    # every pair aligned against the last subject
+    last = np.full(1000, ps.n - 1)
+    hl = np.stack(native.sw_batch_host(ps.q, ps.qoff[:1000], ps.qlen[:1000], ps.s,
+                                       ps.soff[last], ps.slen[last], mat))
+    idx = np.arange(1000)
+    sub = synth.PairSet(ps.q, ps.qoff[idx], ps.qlen[idx], ps.s, ps.soff[last], ps.slen[last], 0)
+    ref = np.stack(oracle.oracle_sw(sub.q, sub.qoff, sub.qlen, sub.s, sub.soff, sub.slen, mat))
+    assert (hl == ref).all()
+
+
 def test_sw_long_queries_multi_stripe(cuda):
     # queries longer than one 1024-row stripe: random, homologous (u8
     # saturation -> i16 pass) and W-runs near / past the 16-bit limit (the
