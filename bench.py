@@ -58,8 +58,9 @@ def parse():
                     help="DB size of the full-search section (proteins)")
     ap.add_argument("--search-queries", type=int, default=10_000,
                     help="queries of the full-search section")
-    ap.add_argument("--search-batch", type=int, default=2500,
-                    help="queries per tpz_search_batch call in the full-search section")
+    ap.add_argument("--search-batch", type=int, default=0,
+                    help="queries per tpz_search_batch call in the full-search sections; 0: an "
+                         "equal share per worker thread (mid size), 2500 (large)")
     ap.add_argument("--no-search", action="store_true",
                     help="skip the full-search (config 2) section")
     return ap.parse_args()
@@ -264,7 +265,7 @@ def large_bench(args, dev):
     load_s = time.perf_counter() - t0
     mat = synth.matrix("BLOSUM62")
     report = {"max_evalue": 1e-3}
-    bsz = args.search_batch
+    bsz = args.search_batch or 2500
     out = {"workload": "full search, large: %d-protein synthetic DB (%.2f G residues, log-normal "
                        "lengths median 300, 50-2000), %d queries of 50-1500 residues (half mutated, "
                        "half random), SEG on, BLOSUM62 11/1, -H 100 -E 1e-3, batches of %d from 2 "
@@ -332,7 +333,9 @@ def search_bench(args, dev):
     load_s = time.perf_counter() - t0
     mat = synth.matrix("BLOSUM62")
     report = {"max_evalue": 1e-3}                     # -H 100 -E 1e-3, ranked on the device
-    bsz = args.search_batch
+    # one batch per worker thread: with more batches than threads the last
+    # batch runs alone on a device the other threads have left idle
+    bsz = args.search_batch or -(-len(q_aa) // args.search_workers)
     # warm-up: one full-size batch per worker thread, so that the device
     # memory pool of every thread has grown to a batch before the timing
     warm = native.prepare_queries(q_aa[:bsz])
