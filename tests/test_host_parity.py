@@ -1,5 +1,6 @@
 """Host-side pieces of the CLI against the reference (CPU only):
-SEG masking, the suffix array, `topaz index` files, blasttab statistics."""
+SEG masking, the suffix array, `topaz index` files, blasttab statistics,
+bitscores and E-values."""
 import ctypes
 import os
 import subprocess
@@ -160,3 +161,24 @@ def test_blasttab_stats_match_reference():
             assert np.float64(o[5].value).tobytes() == np.float64(m.identity).tobytes()
             n += 1
         assert n > 100
+
+
+@pytest.mark.parametrize("variant", ["default", "tight"])
+def test_karlin_matches_reference_golden(golden_search, variant):
+    # bitscore and E-value of every aligned hit (gapless >= 40 goes through
+    # ssw_align; no golden hit reaches the 16-bit drop) as exact doubles
+    g = golden_search
+    hi, hf, meta = g["hitsi_" + variant], g["hitsf_" + variant], g["meta_" + variant]
+    ind = g["ind"].view(np.uint8)
+    nprot = len(ind) // 24
+    db_size = len(g["T"]) - nprot
+    h0, checked = 0, 0
+    for q in range(len(g["qlen"])):
+        nh = int(meta[q][2])
+        for j in range(h0, h0 + nh):
+            if hi[j, 2] == 1 and hi[j, 1] >= 40:
+                bits, ev = native.karlin(int(g["qlen"][q]), db_size, nprot, int(hi[j, 3]))
+                assert (ev, bits) == (hf[j, 0], hf[j, 1]), (q, j, hi[j], hf[j])
+                checked += 1
+        h0 += nh
+    assert checked > 20
