@@ -70,3 +70,24 @@ def test_cli_search_matches_live_reference(cuda, tmp_path, extra):
         outs.append(blocks(r.stdout))
     assert outs[0] == outs[1]
     assert sum(len(v) for v in outs[0][1].values()) > 50
+
+
+@pytest.mark.parametrize("extra", [[], ["--blasttab"]])
+def test_cli_concurrent_batches_print_the_single_thread_output(cuda, tmp_path, extra):
+    # -T 3 with batches of 7 queries keeps three batches in flight on the
+    # device; the lines come out byte for byte as with one thread
+    B.build()
+    prot = synth.protein_db(3000, seed=411)
+    qs = synth.search_queries(prot, 50, 25, seed=412, hi=2000)
+    db_fa, q_fa = str(tmp_path / "db.fa"), str(tmp_path / "q.fa")
+    synth.write_fasta(db_fa, prot)
+    synth.write_fasta(q_fa, qs)
+    pre = str(tmp_path / "db")
+    subprocess.run([B.CLI, "index", "-f", db_fa, "-p", pre], check=True, capture_output=True)
+    outs = []
+    for args in (["-T", "1"], ["-T", "3", "--batch", "7"], ["-T", "4", "--batch", "1"]):
+        r = subprocess.run([B.CLI, "search", "-f", q_fa, "-p", pre, *args, *extra], capture_output=True)
+        assert r.returncode == 0, r.stderr.decode()[-2000:]
+        outs.append(r.stdout)
+    assert outs[0] == outs[1] == outs[2]
+    assert outs[0].count(b"\n") > 50

@@ -202,3 +202,39 @@ def test_search_concurrent_calls_match_sequential(cuda, fresh):
     for a, b in zip(alone, got):
         for k in ("hit_off", "protein", "rawscore", "qend", "send", "bitscore", "evalue", "npops"):
             assert np.array_equal(a[k], b[k]), k
+
+
+def test_index_rejects_bad_text_and_sa(cuda):
+    # both checks run on the device before any kernel reads T[SA[r]] or
+    # indexes the prefix table by a text byte
+    db = make_db(synth.protein_db(60, seed=51))
+    bad_t = dbformat.Database(db.T.copy(), db.SA, db.ind, db.headers)
+    bad_t.T[3] = ord("a")
+    with pytest.raises(native.TopazError, match="internal alphabet"):
+        native.Index(bad_t)
+    bad_sa = dbformat.Database(db.T, db.SA.copy(), db.ind, db.headers)
+    bad_sa.SA[7] = db.Tsize
+    with pytest.raises(native.TopazError, match="SA entry"):
+        native.Index(bad_sa)
+    native.Index(db).close()          # the untouched database still loads
+
+
+def test_index_upload_in_pieces_matches_oracle(cuda):
+    # a text whose SA (8 bytes a row) is over 64 MB goes to the device in
+    # pinned pieces; searches on it match the oracle
+    prot = synth.protein_db(30000, seed=61)
+    db = dbformat.build_from_records([(p.encode(), s) for p, s in zip(prot.ids, prot.seqs)])
+    db.SA = native.sa_build(db.T)
+    assert 8 * db.Tsize > 64 << 20
+    qs = [ab.aa_to_internal(s).tobytes() for s in synth.search_queries(prot, 3, 1, seed=62).seqs]
+    ix = native.Index(db)
+    try:
+        r = ix.search(qs, BLOSUM62)
+    finally:
+        ix.close()
+    opts = oracle.Opts(100, 1e-3, 11, 1, 0.267, 0.041, 0.14, 5, 300000, 5000)
+    for q, qi in enumerate(qs):
+        _, hits, npops, ncnt, nh = oracle.oracle_query(db, qi, BLOSUM62, opts)
+        a, b = int(r["hit_off"][q]), int(r["hit_off"][q + 1])
+        assert (r["npops"][q], r["ncounted"][q], b - a) == (npops, ncnt, nh)
+        assert [int(p) for p in r["protein"][a:b]] == [h.db_index for h in hits]

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "search_internal.cuh"
@@ -85,10 +86,66 @@ struct DevBuf {
     }
 };
 
+// bit 1 of *bad: an SA entry outside [0, Tsize); bit 2: a text byte that is
+// neither '\n' nor an internal-alphabet letter
 __global__ void sa_range_check_kernel(const int64_t *SA, int64_t Tsize, int *bad) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < Tsize;
          i += (int64_t)gridDim.x * blockDim.x)
-        if (SA[i] < 0 || SA[i] >= Tsize) *bad = 1;
+        if (SA[i] < 0 || SA[i] >= Tsize) atomicOr(bad, 1);
+}
+
+__global__ void text_check_kernel(const uint8_t *T, int64_t Tsize, int *bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < Tsize;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t c = T[i];
+        if (c != '\n' && (c < 'A' || c > 'Y')) atomicOr(bad, 2);
+    }
+}
+
+// Host -> device copy of pageable memory (the .psq and .SA file mappings):
+// host threads copy 64 MB pieces into two pinned buffers in turn -- touching
+// the mapping's pages in parallel -- while the previous piece is on its way
+// to the device.
+int upload_pageable(void *dst, const void *src, size_t n) {
+    constexpr size_t kPiece = 64ull << 20;
+    if (n <= kPiece)
+        return cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice) == cudaSuccess
+                   ? TPZ_OK : tpz::cuda_fail(cudaGetLastError(), "index upload");
+    cudaStream_t st = cudaStreamPerThread;
+    uint8_t *pin[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    int rc = TPZ_OK;
+    for (int b = 0; b < 2 && rc == TPZ_OK; ++b)
+        if (cudaHostAlloc((void **)&pin[b], kPiece, cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) != cudaSuccess)
+            rc = tpz::cuda_fail(cudaGetLastError(), "index upload buffers");
+    const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const uint8_t *s8 = (const uint8_t *)src;
+    for (size_t off = 0, k = 0; rc == TPZ_OK && off < n; off += kPiece, ++k) {
+        const size_t len = std::min(kPiece, n - off);
+        uint8_t *buf = pin[k & 1];
+        if (k >= 2 && cudaEventSynchronize(done[k & 1]) != cudaSuccess) {
+            rc = tpz::cuda_fail(cudaGetLastError(), "index upload");
+            break;
+        }
+        const size_t part = (len + nt - 1) / nt;
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt && (size_t)t * part < len; ++t) {
+            const size_t a = (size_t)t * part, e = std::min(len, a + part);
+            th.emplace_back([=] { memcpy(buf + a, s8 + off + a, e - a); });
+        }
+        for (std::thread &x : th) x.join();
+        if (cudaMemcpyAsync((uint8_t *)dst + off, buf, len, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaEventRecord(done[k & 1], st) != cudaSuccess)
+            rc = tpz::cuda_fail(cudaGetLastError(), "index upload");
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess && rc == TPZ_OK)
+        rc = tpz::cuda_fail(cudaGetLastError(), "index upload");
+    for (int b = 0; b < 2; ++b) {
+        if (done[b]) cudaEventDestroy(done[b]);
+        if (pin[b]) cudaFreeHost(pin[b]);
+    }
+    return rc;
 }
 
 struct PackArgs {
@@ -546,13 +603,6 @@ int tpz_index_create(const uint8_t *T, int64_t Tsize, const int64_t *SA, const v
         return TPZ_E_ARG;
     }
     pstart[Psize] = Tsize;
-    for (int64_t i = 0; i < Tsize; ++i) {
-        const uint8_t c = T[i];
-        if (c != '\n' && (c < 'A' || c > 'Y')) {
-            tpz::set_error("tpz_index_create: text byte outside the internal alphabet");
-            return TPZ_E_ARG;
-        }
-    }
 
     tpz_index *ix = new tpz_index();
     TPZ_CUDA(cudaGetDevice(&ix->dev));
@@ -567,20 +617,26 @@ int tpz_index_create(const uint8_t *T, int64_t Tsize, const int64_t *SA, const v
     if ((rc = dalloc(ix, (void **)&dnl, (nblocks + 1) * 4))) return fail(rc);
     if ((rc = dalloc(ix, (void **)&dlb, (kCodes + 1) * 8))) return fail(rc);
     if (cudaMemset(dT + Tsize, '\n', 128) != cudaSuccess ||
-        cudaMemcpy(dT, T, Tsize, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(dSA, 0, sa_rows * 8) != cudaSuccess ||
-        cudaMemcpy(dSA, SA, Tsize * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(dSA + Tsize, 0, (sa_rows - Tsize) * 8) != cudaSuccess ||
         cudaMemcpy(dps, pstart.data(), (Psize + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create copies"));
+    if ((rc = upload_pageable(dT, T, Tsize)) || (rc = upload_pageable(dSA, SA, Tsize * 8)))
+        return fail(rc);
     int *dbad;
     if ((rc = dalloc(ix, (void **)&dbad, 4))) return fail(rc);
     cudaMemset(dbad, 0, 4);
     const int nsm = tpz::sm_count();
-    // every SA entry must index T before any kernel dereferences T[SA[r]]
+    // every text byte must be a letter or '\n' (the prefix table indexes by
+    // letter) and every SA entry must index T, before any kernel reads them
+    text_check_kernel<<<nsm * 8, 256>>>(dT, Tsize, dbad);
     sa_range_check_kernel<<<nsm * 8, 256>>>(dSA, Tsize, dbad);
     int bad = 0;
     if (cudaMemcpy(&bad, dbad, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
-        return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create SA check"));
+        return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create checks"));
+    if (bad & 2) {
+        tpz::set_error("tpz_index_create: text byte outside the internal alphabet");
+        return fail(TPZ_E_ARG);
+    }
     if (bad) {
         tpz::set_error("tpz_index_create: SA entry outside [0, Tsize)");
         return fail(TPZ_E_ARG);

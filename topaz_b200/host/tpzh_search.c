@@ -11,6 +11,12 @@
  * E-values come from tpz_karlin (the C library's log/exp, same expression
  * order).  Queries print in input order; the reference prints them in
  * completion order of its threads, so parity is per-query block.
+ *
+ * -T N runs min(N, 4) host threads, each with one query batch on the device
+ * at a time (the library runs every calling thread on its own CUDA stream),
+ * so one batch's SW overlaps another's walk and the FASTA reading, SEG and
+ * output formatting of the others.  Each batch formats its lines into a
+ * buffer and the buffers are written in batch order.
  */
 #define _GNU_SOURCE
 #include "tpzh.h"
@@ -20,6 +26,7 @@
 #include <fcntl.h>
 #include <inttypes.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -102,6 +109,170 @@ typedef struct {
     int len;
 } query_t;
 
+typedef struct { uint64_t hs, ps; int32_t hl, pl; } rec_t;
+
+#define TPZH_MAX_WORKERS 4
+
+/* What the worker threads of one `topaz search` share. */
+typedef struct {
+    const tpzh_options *o;
+    tpz_index *ix;
+    const tpz_search_opts *so;
+    int report;
+    const int8_t *mat;
+    const rec_t *recs;
+    const char *T, *phr;
+    uint64_t db_size, db_proteins;
+    int64_t B;
+    int prep_threads;
+    tpzh_fasta *f;
+    pthread_mutex_t mu;         /* the reader, the print turn and the totals */
+    pthread_cond_t turn;
+    int64_t next_read, next_print;
+    int done;
+    uint64_t nonzero, total_hits;
+} search_ctx;
+
+/* One batch: SEG + alphabet, the device search, then the lines of every
+ * query into `out`. */
+static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint64_t *nonzero,
+                         uint64_t *total_hits) {
+    const tpzh_options *o = c->o;
+    const int report = c->report;
+    int64_t total = 0;
+    int64_t *qoff = malloc(sizeof(int64_t) * nq);
+    int32_t *qlen = malloc(sizeof(int32_t) * nq);
+    for (int64_t i = 0; i < nq; ++i) { qoff[i] = total; qlen[i] = qs[i].len; total += qs[i].len; }
+    char *cat = malloc(total + 1);
+    for (int64_t i = 0; i < nq; ++i) memcpy(cat + qoff[i], qs[i].seq, qs[i].len);
+    /* run_seg + seq_2internal for the whole batch over host threads */
+    tpz_prepare_queries(cat, qoff, qlen, nq, o->seg_enabled, c->prep_threads);
+    for (int64_t i = 0; i < nq; ++i) memcpy(qs[i].seq, cat + qoff[i], qs[i].len);
+    tpz_search_result *res = NULL;
+    if (tpz_search_batch(c->ix, cat, qoff, qlen, nq, c->so, &res) != 0) {
+        fprintf(stderr, "Error: %s\n", tpz_last_error());
+        exit(EXIT_FAILURE);
+    }
+    int64_t maxh = 1;
+    for (int64_t q = 0; q < nq; ++q) {
+        const int64_t nh = res->hit_off[q + 1] - res->hit_off[q];
+        if (nh > maxh) maxh = nh;
+    }
+    ranked_t *rk = malloc(sizeof(ranked_t) * maxh), *tmp = malloc(sizeof(ranked_t) * maxh);
+    for (int64_t q = 0; q < nq; ++q) {
+        if (res->status[q] & TPZ_Q_SA_END)
+            fprintf(stderr, "Warning: %.*s reached the end of the suffix array (the reference reads past its mapping there)\n",
+                    qs[q].id_len, qs[q].id);
+        const int64_t a = res->hit_off[q], b = res->hit_off[q + 1];
+        int64_t n = 0;
+        if (report) {
+            /* already ranked, cut to -H and to -E */
+            for (int64_t h = a; h < b; ++h) {
+                rk[n].idx = h; rk[n].bits = res->bitscore[h]; rk[n].evalue = res->evalue[h]; n++;
+            }
+        } else
+        for (int64_t h = a; h < b; ++h) {
+            const int st = res->sw_status[h];
+            if (st == TPZ_SW_OK) {
+                rk[n].idx = h;
+                tpz_karlin(qs[q].len, c->db_size, c->db_proteins, o->lambda, o->k, o->H, res->rawscore[h],
+                           &rk[n].bits, &rk[n].evalue);
+                n++;
+            } else if (st == TPZ_SW_GAPLESS_LOW) {
+                rk[n].idx = h; rk[n].bits = 0; rk[n].evalue = 1000; n++;
+            }
+        }
+        if (!report) {
+            stable_sort_bits(rk, n, tmp);
+            if (n > o->num_hits) n = o->num_hits;
+        }
+        int count = 0;
+        int8_t *qidx = NULL;
+        for (int64_t i = 0; i < n; ++i) {
+            if (!(rk[i].evalue <= o->evalue)) continue;
+            const int64_t h = rk[i].idx;
+            const rec_t *pr = &c->recs[res->protein[h]];
+            const char *sid;
+            const int sl = tpzh_header_id(c->phr + pr->hs, pr->hl, &sid);
+            if (o->superfast) {
+                fprintf(out, "%.*s\t%.*s\t%.3e\t%d\n", qs[q].id_len, qs[q].id, sl, sid, rk[i].evalue,
+                        (int)rk[i].bits);
+            } else {
+                tpzh_stats stt;
+                memset(&stt, 0, sizeof stt);
+                if (res->sw_status[h] == TPZ_SW_OK) {
+                    if (!qidx) {
+                        qidx = malloc(qs[q].len + 1);
+                        for (int j = 0; j < qs[q].len; ++j) qidx[j] = g_int2idx[(int)qs[q].seq[j] & 127];
+                    }
+                    int8_t *sidx = malloc(pr->pl + 1);
+                    for (int j = 0; j < pr->pl; ++j) sidx[j] = g_int2idx[(int)c->T[pr->ps + j] & 127];
+                    tpzh_align_stats(qidx, qs[q].len, sidx, pr->pl, c->mat, o->gap_open, o->gap_extend,
+                                     res->qend[h], res->send[h], res->rawscore[h], &stt);
+                    free(sidx);
+                } else {
+                    stt.qstart = stt.sstart = -1;
+                    stt.length = stt.mismatch = stt.gapopen = -1;
+                    stt.identity = INFINITY;
+                }
+                fprintf(out, "%.*s\t%.*s\t%.2f\t%d\t%d\t%d\t%d\t%d\t%d\t%d\t%.3e\t%d\n", qs[q].id_len,
+                        qs[q].id, sl, sid, stt.identity * 100, stt.length, stt.mismatch, stt.gapopen,
+                        stt.qstart + 1, res->qend[h] + 1, stt.sstart + 1, res->send[h] + 1,
+                        rk[i].evalue, (int)rk[i].bits);
+            }
+            ++count;
+        }
+        free(qidx);
+        if (count) { (*nonzero)++; *total_hits += count; }
+    }
+    free(rk); free(tmp);
+    tpz_search_result_free(res);
+    free(cat); free(qoff); free(qlen);
+}
+
+/* Worker: take the next batch from the FASTA reader (batch ids in reading
+ * order), search and format it, then write it when every earlier batch has
+ * been written. */
+static void *search_worker(void *arg) {
+    search_ctx *c = arg;
+    query_t *qs = calloc(c->B, sizeof(query_t));
+    for (;;) {
+        int64_t nq = 0, id = -1;
+        pthread_mutex_lock(&c->mu);
+        while (!c->done && nq < c->B) {
+            tpzh_record r;
+            const int rc = tpzh_fasta_next(c->f, &r);
+            if (rc < 0) exit(EXIT_FAILURE);
+            if (rc == 0) { c->done = 1; break; }
+            qs[nq].id = r.id; qs[nq].id_len = r.id_len;
+            qs[nq].seq = r.seq; qs[nq].len = r.seq_len;
+            nq++;
+        }
+        if (nq) id = c->next_read++;
+        pthread_mutex_unlock(&c->mu);
+        if (nq == 0) break;
+        char *buf = NULL;
+        size_t len = 0;
+        FILE *out = open_memstream(&buf, &len);
+        if (!out) { fprintf(stderr, "Error: %s\n", strerror(errno)); exit(EXIT_FAILURE); }
+        uint64_t nonzero = 0, total_hits = 0;
+        search_batch(c, qs, nq, out, &nonzero, &total_hits);
+        fclose(out);
+        for (int64_t i = 0; i < nq; ++i) { free(qs[i].id); free(qs[i].seq); }
+        pthread_mutex_lock(&c->mu);
+        while (c->next_print != id) pthread_cond_wait(&c->turn, &c->mu);
+        fwrite(buf, 1, len, stdout);
+        c->next_print++;
+        c->nonzero += nonzero;
+        c->total_hits += total_hits;
+        pthread_cond_broadcast(&c->turn);
+        pthread_mutex_unlock(&c->mu);
+        free(buf);
+    }
+    free(qs);
+    return NULL;
+}
+
 int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     struct timeval t0, t1;
     gettimeofday(&t0, NULL);
@@ -147,7 +318,6 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         return -1;
     }
-    typedef struct { uint64_t hs, ps; int32_t hl, pl; } rec_t;
     const rec_t *recs = (const rec_t *)ind.data;
     init_int2idx();
 
@@ -156,10 +326,6 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
 
     tpzh_fasta f;
     if (tpzh_fasta_open(&f, fasta) != 0) exit(EXIT_FAILURE);
-    const int64_t B = o->batch > 0 ? o->batch : 2000;
-    query_t *qs = calloc(B, sizeof(query_t));
-    uint64_t nonzero = 0, total_hits = 0;
-    int done = 0;
     tpz_search_opts so;
     memset(&so, 0, sizeof so);
     so.num_hits = o->num_hits;
@@ -181,113 +347,31 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
         so.db_size = db_size;
         so.db_proteins = db_proteins;
     }
-    while (!done) {
-        int64_t nq = 0;
-        tpzh_record r;
-        while (nq < B) {
-            const int rc = tpzh_fasta_next(&f, &r);
-            if (rc < 0) exit(EXIT_FAILURE);
-            if (rc == 0) { done = 1; break; }
-            qs[nq].id = r.id; qs[nq].id_len = r.id_len;
-            qs[nq].seq = r.seq; qs[nq].len = r.seq_len;
-            nq++;
-        }
-        if (nq == 0) break;
-        int64_t total = 0;
-        int64_t *qoff = malloc(sizeof(int64_t) * nq);
-        int32_t *qlen = malloc(sizeof(int32_t) * nq);
-        for (int64_t i = 0; i < nq; ++i) { qoff[i] = total; qlen[i] = qs[i].len; total += qs[i].len; }
-        char *cat = malloc(total + 1);
-        for (int64_t i = 0; i < nq; ++i) memcpy(cat + qoff[i], qs[i].seq, qs[i].len);
-        /* run_seg + seq_2internal for the whole batch over host threads */
-        const long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-        tpz_prepare_queries(cat, qoff, qlen, nq, o->seg_enabled, ncpu > 0 ? (int)ncpu : 1);
-        for (int64_t i = 0; i < nq; ++i) memcpy(qs[i].seq, cat + qoff[i], qs[i].len);
-        tpz_search_result *res = NULL;
-        if (tpz_search_batch(ix, cat, qoff, qlen, nq, &so, &res) != 0) {
-            fprintf(stderr, "Error: %s\n", tpz_last_error());
+    int nw = o->num_threads < 1 ? 1 : o->num_threads;
+    if (nw > TPZH_MAX_WORKERS) nw = TPZH_MAX_WORKERS;
+    const long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    search_ctx c;
+    memset(&c, 0, sizeof c);
+    c.o = o; c.ix = ix; c.so = &so; c.report = report; c.mat = mat; c.recs = recs;
+    c.T = T.data; c.phr = phr.data; c.db_size = db_size; c.db_proteins = db_proteins;
+    c.B = o->batch > 0 ? o->batch : 2000;
+    c.prep_threads = ncpu > nw ? (int)(ncpu / nw) : 1;
+    c.f = &f;
+    pthread_mutex_init(&c.mu, NULL);
+    pthread_cond_init(&c.turn, NULL);
+    pthread_t th[TPZH_MAX_WORKERS];
+    for (int i = 1; i < nw; ++i)
+        if (pthread_create(&th[i], NULL, search_worker, &c) != 0) {
+            fprintf(stderr, "Error: could not start a search thread\n");
             exit(EXIT_FAILURE);
         }
-        int64_t maxh = 1;
-        for (int64_t q = 0; q < nq; ++q) {
-            const int64_t nh = res->hit_off[q + 1] - res->hit_off[q];
-            if (nh > maxh) maxh = nh;
-        }
-        ranked_t *rk = malloc(sizeof(ranked_t) * maxh), *tmp = malloc(sizeof(ranked_t) * maxh);
-        for (int64_t q = 0; q < nq; ++q) {
-            if (res->status[q] & TPZ_Q_SA_END)
-                fprintf(stderr, "Warning: %.*s reached the end of the suffix array (the reference reads past its mapping there)\n",
-                        qs[q].id_len, qs[q].id);
-            const int64_t a = res->hit_off[q], b = res->hit_off[q + 1];
-            int64_t n = 0;
-            if (report) {
-                /* already ranked, cut to -H and to -E */
-                for (int64_t h = a; h < b; ++h) {
-                    rk[n].idx = h; rk[n].bits = res->bitscore[h]; rk[n].evalue = res->evalue[h]; n++;
-                }
-            } else
-            for (int64_t h = a; h < b; ++h) {
-                const int st = res->sw_status[h];
-                if (st == TPZ_SW_OK) {
-                    rk[n].idx = h;
-                    tpz_karlin(qs[q].len, db_size, db_proteins, o->lambda, o->k, o->H, res->rawscore[h],
-                               &rk[n].bits, &rk[n].evalue);
-                    n++;
-                } else if (st == TPZ_SW_GAPLESS_LOW) {
-                    rk[n].idx = h; rk[n].bits = 0; rk[n].evalue = 1000; n++;
-                }
-            }
-            if (!report) {
-                stable_sort_bits(rk, n, tmp);
-                if (n > o->num_hits) n = o->num_hits;
-            }
-            int count = 0;
-            int8_t *qidx = NULL;
-            for (int64_t i = 0; i < n; ++i) {
-                if (!(rk[i].evalue <= o->evalue)) continue;
-                const int64_t h = rk[i].idx;
-                const rec_t *pr = &recs[res->protein[h]];
-                const char *sid;
-                const int sl = tpzh_header_id(phr.data + pr->hs, pr->hl, &sid);
-                if (o->superfast) {
-                    printf("%.*s\t%.*s\t%.3e\t%d\n", qs[q].id_len, qs[q].id, sl, sid, rk[i].evalue,
-                           (int)rk[i].bits);
-                } else {
-                    tpzh_stats stt;
-                    memset(&stt, 0, sizeof stt);
-                    if (res->sw_status[h] == TPZ_SW_OK) {
-                        if (!qidx) {
-                            qidx = malloc(qs[q].len + 1);
-                            for (int j = 0; j < qs[q].len; ++j) qidx[j] = g_int2idx[(int)qs[q].seq[j] & 127];
-                        }
-                        int8_t *sidx = malloc(pr->pl + 1);
-                        for (int j = 0; j < pr->pl; ++j) sidx[j] = g_int2idx[(int)T.data[pr->ps + j] & 127];
-                        tpzh_align_stats(qidx, qs[q].len, sidx, pr->pl, mat, o->gap_open, o->gap_extend,
-                                         res->qend[h], res->send[h], res->rawscore[h], &stt);
-                        free(sidx);
-                    } else {
-                        stt.qstart = stt.sstart = -1;
-                        stt.length = stt.mismatch = stt.gapopen = -1;
-                        stt.identity = INFINITY;
-                    }
-                    printf("%.*s\t%.*s\t%.2f\t%d\t%d\t%d\t%d\t%d\t%d\t%d\t%.3e\t%d\n", qs[q].id_len, qs[q].id,
-                           sl, sid, stt.identity * 100, stt.length, stt.mismatch, stt.gapopen,
-                           stt.qstart + 1, res->qend[h] + 1, stt.sstart + 1, res->send[h] + 1,
-                           rk[i].evalue, (int)rk[i].bits);
-                }
-                ++count;
-            }
-            free(qidx);
-            if (count) { nonzero++; total_hits += count; }
-        }
-        free(rk); free(tmp);
-        tpz_search_result_free(res);
-        free(cat); free(qoff); free(qlen);
-        for (int64_t i = 0; i < nq; ++i) { free(qs[i].id); free(qs[i].seq); }
-    }
+    search_worker(&c);
+    for (int i = 1; i < nw; ++i) pthread_join(th[i], NULL);
+    pthread_cond_destroy(&c.turn);
+    pthread_mutex_destroy(&c.mu);
+    const uint64_t nonzero = c.nonzero, total_hits = c.total_hits;
     fflush(stdout);
     tpzh_fasta_close(&f);
-    free(qs);
     tpz_index_destroy(ix);
     gettimeofday(&t1, NULL);
     fprintf(stderr, "output %" PRIu64 " hits for %" PRIu64 " queries\n", total_hits, nonzero);
