@@ -133,8 +133,53 @@ typedef struct {
     uint64_t nonzero, total_hits;
 } search_ctx;
 
+/* A --blasttab line: query, hit, ranking values and its statistics. */
+typedef struct {
+    int64_t q, h;
+    double bits, evalue;
+    tpzh_stats st;
+} line_t;
+
+typedef struct {
+    const search_ctx *c;
+    const query_t *qs;
+    const tpz_search_result *res;
+    line_t *lines;
+    int64_t from, to;
+} stats_job;
+
+/* ssw_align_stats (src/ssw_wrapper.c:132-155) of the lines [from, to): one
+ * host thread's share of a batch. */
+static void *stats_worker(void *arg) {
+    const stats_job *j = arg;
+    const search_ctx *c = j->c;
+    const tpz_search_result *res = j->res;
+    for (int64_t i = j->from; i < j->to; ++i) {
+        line_t *ln = &j->lines[i];
+        const int64_t h = ln->h;
+        memset(&ln->st, 0, sizeof ln->st);
+        if (res->sw_status[h] == TPZ_SW_OK) {
+            const query_t *qq = &j->qs[ln->q];
+            const rec_t *pr = &c->recs[res->protein[h]];
+            int8_t *qidx = malloc(qq->len + 1), *sidx = malloc(pr->pl + 1);
+            for (int k = 0; k < qq->len; ++k) qidx[k] = g_int2idx[(int)qq->seq[k] & 127];
+            for (int k = 0; k < pr->pl; ++k) sidx[k] = g_int2idx[(int)c->T[pr->ps + k] & 127];
+            tpzh_align_stats(qidx, qq->len, sidx, pr->pl, c->mat, c->o->gap_open, c->o->gap_extend,
+                             res->qend[h], res->send[h], res->rawscore[h], &ln->st);
+            free(qidx);
+            free(sidx);
+        } else {
+            ln->st.qstart = ln->st.sstart = -1;
+            ln->st.length = ln->st.mismatch = ln->st.gapopen = -1;
+            ln->st.identity = INFINITY;
+        }
+    }
+    return NULL;
+}
+
 /* One batch: SEG + alphabet, the device search, then the lines of every
- * query into `out`. */
+ * query into `out`.  --blasttab statistics (about a millisecond per line)
+ * are computed for the whole batch over host threads before printing. */
 static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint64_t *nonzero,
                          uint64_t *total_hits) {
     const tpzh_options *o = c->o;
@@ -159,6 +204,8 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
         if (nh > maxh) maxh = nh;
     }
     ranked_t *rk = malloc(sizeof(ranked_t) * maxh), *tmp = malloc(sizeof(ranked_t) * maxh);
+    line_t *lines = NULL;
+    int64_t nlines = 0, lcap = 0;
     for (int64_t q = 0; q < nq; ++q) {
         if (res->status[q] & TPZ_Q_SA_END)
             fprintf(stderr, "Warning: %.*s reached the end of the suffix array (the reference reads past its mapping there)\n",
@@ -187,44 +234,63 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
             if (n > o->num_hits) n = o->num_hits;
         }
         int count = 0;
-        int8_t *qidx = NULL;
         for (int64_t i = 0; i < n; ++i) {
             if (!(rk[i].evalue <= o->evalue)) continue;
             const int64_t h = rk[i].idx;
-            const rec_t *pr = &c->recs[res->protein[h]];
-            const char *sid;
-            const int sl = tpzh_header_id(c->phr + pr->hs, pr->hl, &sid);
             if (o->superfast) {
+                const rec_t *pr = &c->recs[res->protein[h]];
+                const char *sid;
+                const int sl = tpzh_header_id(c->phr + pr->hs, pr->hl, &sid);
                 fprintf(out, "%.*s\t%.*s\t%.3e\t%d\n", qs[q].id_len, qs[q].id, sl, sid, rk[i].evalue,
                         (int)rk[i].bits);
             } else {
-                tpzh_stats stt;
-                memset(&stt, 0, sizeof stt);
-                if (res->sw_status[h] == TPZ_SW_OK) {
-                    if (!qidx) {
-                        qidx = malloc(qs[q].len + 1);
-                        for (int j = 0; j < qs[q].len; ++j) qidx[j] = g_int2idx[(int)qs[q].seq[j] & 127];
-                    }
-                    int8_t *sidx = malloc(pr->pl + 1);
-                    for (int j = 0; j < pr->pl; ++j) sidx[j] = g_int2idx[(int)c->T[pr->ps + j] & 127];
-                    tpzh_align_stats(qidx, qs[q].len, sidx, pr->pl, c->mat, o->gap_open, o->gap_extend,
-                                     res->qend[h], res->send[h], res->rawscore[h], &stt);
-                    free(sidx);
-                } else {
-                    stt.qstart = stt.sstart = -1;
-                    stt.length = stt.mismatch = stt.gapopen = -1;
-                    stt.identity = INFINITY;
+                if (nlines == lcap) {
+                    lcap = lcap ? 2 * lcap : 1024;
+                    lines = realloc(lines, sizeof(line_t) * lcap);
+                    if (!lines) { fprintf(stderr, "Error: out of memory\n"); exit(EXIT_FAILURE); }
                 }
-                fprintf(out, "%.*s\t%.*s\t%.2f\t%d\t%d\t%d\t%d\t%d\t%d\t%d\t%.3e\t%d\n", qs[q].id_len,
-                        qs[q].id, sl, sid, stt.identity * 100, stt.length, stt.mismatch, stt.gapopen,
-                        stt.qstart + 1, res->qend[h] + 1, stt.sstart + 1, res->send[h] + 1,
-                        rk[i].evalue, (int)rk[i].bits);
+                line_t *ln = &lines[nlines++];
+                ln->q = q; ln->h = h; ln->bits = rk[i].bits; ln->evalue = rk[i].evalue;
             }
             ++count;
         }
-        free(qidx);
         if (count) { (*nonzero)++; *total_hits += count; }
     }
+    if (nlines) {
+        /* statistics over host threads, then the lines in order */
+        int nt = c->prep_threads < 1 ? 1 : c->prep_threads;
+        if (nt > nlines) nt = (int)nlines;
+        stats_job jobs[64];
+        pthread_t th[64];
+        int running[64] = {0};
+        if (nt > 64) nt = 64;
+        const int64_t per = (nlines + nt - 1) / nt;
+        for (int t = 0; t < nt; ++t) {
+            jobs[t].c = c; jobs[t].qs = qs; jobs[t].res = res; jobs[t].lines = lines;
+            jobs[t].from = t * per < nlines ? t * per : nlines;
+            jobs[t].to = (t + 1) * per < nlines ? (t + 1) * per : nlines;
+        }
+        for (int t = 1; t < nt; ++t) {
+            running[t] = pthread_create(&th[t], NULL, stats_worker, &jobs[t]) == 0;
+            if (!running[t]) stats_worker(&jobs[t]);
+        }
+        stats_worker(&jobs[0]);
+        for (int t = 1; t < nt; ++t)
+            if (running[t]) pthread_join(th[t], NULL);
+        for (int64_t i = 0; i < nlines; ++i) {
+            const line_t *ln = &lines[i];
+            const int64_t q = ln->q, h = ln->h;
+            const rec_t *pr = &c->recs[res->protein[h]];
+            const char *sid;
+            const int sl = tpzh_header_id(c->phr + pr->hs, pr->hl, &sid);
+            const tpzh_stats *st = &ln->st;
+            fprintf(out, "%.*s\t%.*s\t%.2f\t%d\t%d\t%d\t%d\t%d\t%d\t%d\t%.3e\t%d\n", qs[q].id_len,
+                    qs[q].id, sl, sid, st->identity * 100, st->length, st->mismatch, st->gapopen,
+                    st->qstart + 1, res->qend[h] + 1, st->sstart + 1, res->send[h] + 1, ln->evalue,
+                    (int)ln->bits);
+        }
+    }
+    free(lines);
     free(rk); free(tmp);
     tpz_search_result_free(res);
     free(cat); free(qoff); free(qlen);
