@@ -424,35 +424,56 @@ def search_bench(args, dev):
                 while fh.read(64 << 20):
                     pass
 
-        def run(exe, n):
-            fa = os.path.join(tmp, "q%d.fa" % n)
-            synth.write_fasta(fa, synth.Proteins(["q%d" % i for i in range(n)],
-                                                 [np.frombuffer(q, np.uint8) for q in q_aa[:n]]))
+        def run(exe, idx, extra=(), tag="q"):
+            fa = os.path.join(tmp, "%s%d.fa" % (tag, len(idx)))
+            synth.write_fasta(fa, synth.Proteins(["q%d" % i for i in idx],
+                                                 [np.frombuffer(q_aa[i], np.uint8) for i in idx]))
             t = time.perf_counter()
-            r = subprocess.run([exe, "search", "-f", fa, "-p", pre, "-T", str(threads)],
+            r = subprocess.run([exe, "search", "-f", fa, "-p", pre, "-T", str(threads), *extra],
                                capture_output=True, cwd=tmp)
             return time.perf_counter() - t, r
 
-        dt, _ = run(oracle.REF_BIN, 4 * threads)
-        n = int(min(len(q_aa), max(4 * threads, 4 * threads * 15.0 / max(dt, 1e-3))))
-        dt, rr = run(oracle.REF_BIN, n)
-        dt_cli, rm = run(B.CLI, n)
-        dt_cli_all, _ = run(B.CLI, len(q_aa))
+        def spread(n):
+            # n queries evenly spaced over the whole query set, so that the
+            # mutated and the random halves are both represented
+            return np.unique(np.linspace(0, len(q_aa) - 1, n).astype(np.int64)).tolist()
 
         def blocks(text):
             d = {}
             for ln in text.decode().splitlines()[1:]:
                 d.setdefault(ln.split("\t", 1)[0], []).append(ln)
             return d
-        out["cpu_reference"] = {"queries_per_s": round(n / dt, 2), "threads": threads,
-                                "kind": "reference", "sample": "first %d queries, topaz search -T %d, "
-                                "DB files in page cache" % (n, threads)}
-        out["parity_sample"] = {"queries": n, "identical_blocks": blocks(rr.stdout) == blocks(rm.stdout),
-                                "lines": rr.stdout.count(b"\n") - 1}
+
+        dt, _ = run(oracle.REF_BIN, spread(4 * threads))
+        n = int(min(len(q_aa), max(4 * threads, 4 * threads * 15.0 / max(dt, 1e-3))))
+        sample = spread(n)
+        dt, rr = run(oracle.REF_BIN, sample)
+        dt_cli, rm = run(B.CLI, sample)
+        dt_cli_all, _ = run(B.CLI, list(range(len(q_aa))))
+        half = len(q_aa) // 2
+        out["cpu_reference"] = {"queries_per_s": round(len(sample) / dt, 2), "threads": threads,
+                                "kind": "reference", "sample": "%d queries evenly spaced over the %d "
+                                "(%d mutated, %d random), topaz search -T %d, DB files in page cache"
+                                % (len(sample), len(q_aa), sum(i < half for i in sample),
+                                   sum(i >= half for i in sample), threads)}
+        out["parity_sample"] = {"default": {"queries": len(sample),
+                                            "identical_blocks": blocks(rr.stdout) == blocks(rm.stdout),
+                                            "lines": rr.stdout.count(b"\n") - 1}}
+        # --fast and --blasttab on smaller evenly spaced samples, each mode
+        # compared per query block and timed for both binaries
+        for mode, extra, frac in (("fast", ("--fast",), 0.5), ("blasttab", ("--blasttab",), 0.5)):
+            sm = spread(max(4 * threads, int(len(sample) * frac)))
+            dr, r1 = run(oracle.REF_BIN, sm, extra, tag=mode)
+            do, r2 = run(B.CLI, sm, extra, tag=mode)
+            out["parity_sample"][mode] = {
+                "queries": len(sm), "identical_blocks": blocks(r1.stdout) == blocks(r2.stdout),
+                "lines": r1.stdout.count(b"\n") - 1,
+                "reference_queries_per_s": round(len(sm) / dr, 2),
+                "cli_queries_per_s": round(len(sm) / do, 2)}
         # our `topaz search` as a user runs it: process start to exit (CUDA
         # context, index upload, FASTA, SEG, search, output), -T as above
         # (at most 4 batches in flight), on the sample and on all queries
-        out["cli"] = {"queries_per_s_sample": round(n / dt_cli, 1),
+        out["cli"] = {"queries_per_s_sample": round(len(sample) / dt_cli, 1),
                       "queries_per_s_all": round(len(q_aa) / dt_cli_all, 1),
                       "sample_s": round(dt_cli, 2), "all_s": round(dt_cli_all, 2),
                       "threads": threads, "api": "topaz search CLI (whole process)"}
@@ -651,7 +672,11 @@ def native_arm(args, rank, local_rank, world):
                          "frac": round(achieved / peak_gcups, 4),
                          "peak_source": "measured live: __viaddmax_s16x2 issue rate %.3e op/s / %d DPX ops per cell"
                                         % (dpx_ops_s, DPX_OPS_PER_CELL),
-                         "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None)},
+                         "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None),
+                         "traffic_source": ("not measured in this run: DRAM bytes per cell of the "
+                                            "ncu capture in profiles/sw_microbench_traffic.txt "
+                                            "(100,000-pair case), scaled to this step's cells"
+                                            if traffic_per_cell else None)},
             "cpu_baseline": cpu,
             "per_pair_gpu": per_pair,
             "clocks": clk,

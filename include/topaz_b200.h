@@ -72,7 +72,7 @@ TPZ_API int tpz_matrix(const char *name, int8_t *out625);
  * (src/query.c:304-340) / align_using_ssw_profile (src/ssw_wrapper.c:157-245).
  *
  * Pair i: query = q[qoff[i] .. qoff[i]+qlen[i]), subject = s[soff[i] ..
- * soff[i]+slen[i]).  Limits: 1 <= qlen <= TPZ_SW_MAX_QLEN, 0 <= slen <=
+ * soff[i]+slen[i]).  Limits: 1 <= qlen <= TPZ_SW_MAX_QLEN, 0 <= slen <
  * TPZ_SW_MAX_SLEN, gap_open > gap_extend >= 0, gap_open <= 255.
  * Outputs per pair: score, ref_end (0-based subject end, -1 when score is 0),
  * read_end (0-based query end), status (TPZ_SW_*).
@@ -108,8 +108,11 @@ TPZ_API int tpz_sw_align_one(const int8_t *q, int32_t qlen, const int8_t *s, int
  * through a request, or a loop that cannot afford the device-wide
  * synchronization of cudaMalloc/cudaFree.  Same arguments and results as
  * tpz_sw_batch_device; at most TPZ_SW_NOALLOC_MAX_PAIRS pairs per call
- * (TPZ_E_RANGE beyond) and queries of at most TPZ_SW_NOALLOC_MAX_QLEN
- * residues (longer ones get status TPZ_SW_INVALID).  Scratch is one static device array per device
+ * (TPZ_E_RANGE beyond), queries of at most TPZ_SW_NOALLOC_MAX_QLEN
+ * residues (longer ones get status TPZ_SW_INVALID) and matrices whose
+ * largest entry is at most TPZ_SW_NOALLOC_MAX_ENTRY (TPZ_E_ARG beyond: such
+ * scores can pass the 16-bit range, and the allocating call's 32-bit rerun
+ * needs scratch of its own).  Scratch is one static device array per device
  * (about 0.6 MB, held until the process exits) shared by all calls: calls
  * whose work overlaps on the GPU (other streams or threads) race on it, so
  * order them on one stream.  All work goes to `stream`; nothing is
@@ -118,6 +121,7 @@ TPZ_API int tpz_sw_align_one(const int8_t *q, int32_t qlen, const int8_t *s, int
  * before any stream capture that includes a call. */
 #define TPZ_SW_NOALLOC_MAX_PAIRS 65536
 #define TPZ_SW_NOALLOC_MAX_QLEN 1024
+#define TPZ_SW_NOALLOC_MAX_ENTRY 31
 TPZ_API int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int64_t *qoff,
                                         const int32_t *qlen, const int8_t *s, const int64_t *soff,
                                         const int32_t *slen, const int8_t *mat625_host,
@@ -158,6 +162,33 @@ TPZ_API int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_
                              const int32_t *qlen, int64_t nq, const int32_t *query_of,
                              const int32_t *qoffset, const int64_t *row, int64_t n,
                              const int8_t *mat625, int32_t *score, int32_t *length);
+
+/* Per-call forms of the two seams, with the argument lists of
+ * src/search.h:13-14: the resident index stands in for db_t (its T, SA and
+ * Tsize), the query's residues and length for seq_t, the substitution
+ * matrix for options_t (the one option sa_hsp reads).  Each call is one
+ * small launch that waits for its result -- for parity tests and for
+ * per-call sites; the batch forms above are the fast path.
+ *
+ * tpz_sa_search (sa_search, src/search.c:237-362): pattern = q[offset ..
+ * offset + length), or to the end of q when length <= 0.  idx = the first row
+ * whose suffix starts with the pattern if one does, else the lower bound;
+ * num_matches = the number of rows starting with it; last_position = the
+ * common prefix length with the last row the reference's first binary
+ * search compares (the pattern length when a row starts with it).  Returns
+ * 0, or -1 (with *idx = -1) for an empty pattern or index, as sa_search
+ * does; TPZ_E_ARG for bytes outside 'A'..'Y'. */
+TPZ_API int tpz_sa_search(const tpz_index *db, const char *q, int32_t qlen, int64_t offset,
+                          int64_t length, int64_t *idx, int64_t *num_matches,
+                          int64_t *last_position);
+/* tpz_sa_hsp (sa_hsp, src/search.c:99-190): gapless extension of query
+ * offset qoffset against SA row `position`; gapless_length -1 when the first
+ * symbols differ, -2 for a row outside the readable SA (where sa_hsp reads
+ * past its mapping).  Returns 0 as sa_hsp does, or a TPZ_E* code for bad
+ * arguments (0 <= qoffset < qlen). */
+TPZ_API int tpz_sa_hsp(const tpz_index *db, const char *q, int32_t qlen, int32_t qoffset,
+                       int64_t position, const int8_t *mat625, int32_t *gapless_score,
+                       int32_t *gapless_length);
 
 /* ------------------------------------------------------------------------
  * Whole queries: seed lookup, best-first SA walk into the capped hitlist

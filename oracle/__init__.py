@@ -19,7 +19,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libtopazref.so")
 REF_BIN = os.path.join(HERE, "_ref", "topaz")
-REF_SRC = "/root/reference/src"
+# the TOPAZ source tree (its src/ directory) to compile the reference checker
+# from; unset where the sources are not present (a host that only runs the
+# prebuilt _ref/)
+REF_SRC = os.environ.get("TOPAZ_REF_SRC", "")
 
 _VP = ctypes.c_void_p
 _orc = None
@@ -33,9 +36,12 @@ def build_oracle():
 def build_ref():
     """Compiles the reference sources where they lie (development container
     only).  Returns False when the sources are not present."""
-    if not os.path.isdir(REF_SRC):
+    if not REF_SRC or not os.path.isdir(REF_SRC):
         return False
-    subprocess.check_call(["make", "-s", "-C", HERE, "-j8", "ref"])
+    subprocess.check_call(["make", "-s", "-C", HERE, "-j8", "ref", "REF=" + REF_SRC])
+    # the reference's ssw_wrapper.c relinked against the library (needs
+    # libtopaz_b200.so built first)
+    subprocess.check_call(["make", "-s", "-C", HERE, "relink", "REF=" + REF_SRC])
     return True
 
 

@@ -240,6 +240,19 @@ void ref_seed_list(void *dbh, const char *qint, int qlen, int min_hit_length,
     seq_free(q);
 }
 
+/* One sa_search call (src/search.c:237-362) with all three outputs; returns
+ * its return value. */
+int ref_sa_search(void *dbh, const char *qint, int qlen, int64_t offset, int64_t length,
+                  int64_t *idx, int64_t *num_matches, int64_t *last_position) {
+    ref_db_t *r = (ref_db_t *)dbh;
+    seq_t *q = make_query(qint, qlen);
+    saidx64_t p = -7, nm = -7, lp = -7;
+    int rc = sa_search(&r->db, q, offset, length, &p, &nm, &lp);
+    *idx = p; *num_matches = nm; *last_position = lp;
+    seq_free(q);
+    return rc;
+}
+
 /* One sa_hsp call (src/search.c:99-190) at SA row `row`, query offset off. */
 void ref_hsp(void *dbh, const char *qint, int qlen, int off, int64_t row, const char *matrix,
              int32_t *score, int32_t *len) {

@@ -83,3 +83,43 @@ def test_noalloc_rejects_batches_above_its_limit(cuda):
     assert rc == -4
     assert b"exceed" in native.lib().tpz_last_error()
     assert (got == -7).all()                          # nothing was written
+
+
+def test_noalloc_matches_oracle_and_marks_long_queries_invalid(cuda):
+    # checked against the CPU restatement of ssw_align directly, with queries
+    # on both sides of the 1,024-residue limit of the fixed scratch
+    import oracle
+    torch = cuda
+    mat = synth.matrix("BLOSUM62")
+    ps = synth.sw_pairs(600, seed=91, q_median=900, q_range=(1, 1300), s_range=(0, 1200))
+    t = _device_pairs(torch, ps)
+    rc, got = _call_noalloc(torch, t, ps.n, mat)
+    assert rc == 0, native.lib().tpz_last_error()
+    long_q = ps.qlen > 1024
+    assert long_q.sum() > 50 and (~long_q).sum() > 300
+    assert (got[3][long_q] == native.TPZ_SW_INVALID).all()
+    ok = np.flatnonzero(~long_q)
+    ref = np.stack(oracle.oracle_sw(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat, 11, 1))
+    assert (got[:, ok] == ref[:, ok]).all()
+
+
+def test_noalloc_rejects_matrices_beyond_16_bit_range(cuda):
+    # largest entry 32: a 1,024-residue query could score past what the
+    # 16-bit lanes hold exactly; 31 is still accepted and equals the
+    # allocating call (which would re-run such scores in 32 bits)
+    torch = cuda
+    ps = synth.sw_pairs(300, seed=12, q_range=(900, 1024), s_range=(900, 1100))
+    t = _device_pairs(torch, ps)
+    for diag, want in ((32, -1), (31, 0)):
+        mat = np.full((25, 25), -3, np.int8)
+        np.fill_diagonal(mat, diag)
+        rc, got = _call_noalloc(torch, t, ps.n, mat)
+        assert rc == want, native.lib().tpz_last_error()
+        if rc:
+            assert b"largest matrix entry" in native.lib().tpz_last_error()
+            assert (got == -7).all()
+            continue
+        native.sw_batch_torch(t, mat, 11, 1)
+        torch.cuda.synchronize()
+        ref = np.stack([t[k].cpu().numpy() for k in _FIELDS])
+        assert (got == ref).all()

@@ -740,6 +740,49 @@ int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     return TPZ_OK;
 }
 
+int tpz_sa_search(const tpz_index *db, const char *q, int32_t qlen, int64_t offset, int64_t length,
+                  int64_t *idx, int64_t *num_matches, int64_t *last_position) {
+    // sa_search's own argument checks and return value (src/search.c:276-278)
+    if (idx) *idx = -1;
+    const int64_t m = length > 0 ? length : (int64_t)qlen - offset;
+    if (!db || !q || db->d.Tsize <= 0 || m <= 0 || offset < 0 || offset + m > qlen) {
+        tpz::set_error("tpz_sa_search: empty pattern or index, or span outside the query");
+        return -1;
+    }
+    if (!letters_ok(q + offset, m)) {
+        tpz::set_error("tpz_sa_search: pattern must be internal letters 'A'..'Y'");
+        return TPZ_E_ARG;
+    }
+    DevBuf b;
+    uint8_t *dp;
+    int64_t *dout;
+    int rc;
+    if ((rc = b.alloc(&dp, m)) || (rc = b.alloc(&dout, 3))) return rc;
+    cudaStream_t st = cudaStreamPerThread;
+    TPZ_CUDA(cudaMemcpyAsync(dp, q + offset, m, cudaMemcpyHostToDevice, st));
+    tpz::search::sa_search_call_kernel<<<1, 1, 0, st>>>(db->d, dp, m, dout);
+    TPZ_CUDA(cudaGetLastError());
+    int64_t h[3];
+    TPZ_CUDA(cudaMemcpyAsync(h, dout, sizeof h, cudaMemcpyDeviceToHost, st));
+    TPZ_CUDA(cudaStreamSynchronize(st));
+    if (idx) *idx = h[0];
+    if (num_matches) *num_matches = h[1];
+    if (last_position) *last_position = h[2];
+    return 0;
+}
+
+int tpz_sa_hsp(const tpz_index *db, const char *q, int32_t qlen, int32_t qoffset, int64_t position,
+               const int8_t *mat625, int32_t *gapless_score, int32_t *gapless_length) {
+    if (!gapless_score || !gapless_length) {
+        tpz::set_error("tpz_sa_hsp: NULL output");
+        return TPZ_E_ARG;
+    }
+    const int64_t qo = 0;
+    const int32_t qf = 0;
+    return tpz_sa_hsp_batch(db, q, &qo, &qlen, 1, &qf, &qoffset, &position, 1, mat625,
+                            gapless_score, gapless_length);
+}
+
 int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
                      const int32_t *qlen, int64_t nq, const tpz_search_opts *o,
                      tpz_search_result **out) {

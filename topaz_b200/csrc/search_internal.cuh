@@ -93,6 +93,7 @@ __global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t
                                  int32_t *len);
 __global__ void lower_bound_kernel(DevIndex ix, const uint8_t *pcat, const int64_t *poff,
                                    const int32_t *plen, int64_t n, int64_t *out);
+__global__ void sa_search_call_kernel(DevIndex ix, const uint8_t *P, int64_t m, int64_t *out3);
 
 }  // namespace search
 
@@ -104,7 +105,12 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
-                   int score_only, const int32_t *subset = nullptr, int64_t nsub = 0);
+                   int score_only, const int32_t *subset = nullptr, int64_t nsub = 0,
+                   int known_multi_maxn = -1);
+// known_multi_maxn >= 0: the caller knows the longest subject among pairs
+// with queries longer than one 1,024-row stripe (0: no such pair), so the
+// call need not read it back from the device before sizing the stripe
+// boundary buffer (no host wait inside the call).
 // The same for pairs grouped by query (group g = pairs [gstart[g],
 // gstart[g+1]), all with query length gqlen[g]): groups with enough pairs go
 // to the query-major kernels, one shared profile per query; the rest by pair.

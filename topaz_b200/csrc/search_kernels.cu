@@ -273,6 +273,66 @@ __global__ void lower_bound_kernel(DevIndex ix, const uint8_t *pcat, const int64
         out[g] = lower_bound(ix, pcat + poff[g], plen[g]);
 }
 
+// The per-call sa_search (src/search.c:237-362) in one thread, with all
+// three of its outputs.  The lower bound and the match count have one answer
+// each, whatever the search; `last_position` is the common prefix length of
+// P with the last row the reference's binary search compares in its first
+// loop (P's length once a row starting with P is found), so this search
+// probes the rows in that same order: the window [lo, lo + size) with its
+// probe at lo + half, both halves' known prefix lengths carried (a suffix
+// between two rows shares at least the smaller of their common prefixes with
+// P, so comparisons start past it).
+__device__ int cmp_from(const DevIndex &ix, int64_t suf, const uint8_t *P, int64_t m,
+                        int64_t *match) {
+    int64_t i = suf + *match, j = *match;
+    int r = 0;
+    while (i < ix.Tsize && j < m && (r = (int)ix.T[i] - (int)P[j]) == 0) { ++i; ++j; }
+    *match = j;
+    return r == 0 ? -(j != m) : r;
+}
+
+__global__ void sa_search_call_kernel(DevIndex ix, const uint8_t *P, int64_t m, int64_t *out3) {
+    int64_t lo = 0, size = ix.Tsize, half = size >> 1, lm = 0, rm = 0, match = 0;
+    bool found = false;
+    while (size > 0) {
+        match = lm < rm ? lm : rm;
+        const int r = cmp_from(ix, ix.SA[lo + half], P, m, &match);
+        if (r < 0) {
+            lo += half + 1;
+            half -= (size & 1) ^ 1;
+            lm = match;
+        } else if (r > 0) {
+            rm = match;
+        } else {
+            found = true;
+            break;
+        }
+        size = half;
+        half >>= 1;
+    }
+    int64_t first = lo, count = 0;
+    if (found) {
+        // rows starting with P form one run: its first row, then its end
+        int64_t a = 0, b = ix.Tsize;
+        while (a < b) {
+            const int64_t mid = a + ((b - a) >> 1);
+            int64_t k = 0;
+            if (cmp_from(ix, ix.SA[mid], P, m, &k) < 0) a = mid + 1; else b = mid;
+        }
+        first = a;
+        b = ix.Tsize;
+        while (a < b) {
+            const int64_t mid = a + ((b - a) >> 1);
+            int64_t k = 0;
+            if (cmp_from(ix, ix.SA[mid], P, m, &k) == 0) a = mid + 1; else b = mid;
+        }
+        count = a - first;
+    }
+    out3[0] = first;
+    out3[1] = count;
+    out3[2] = match;
+}
+
 // One thread per (row, query offset) for the stage entry point.
 __global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t *qoff,
                                  const int32_t *qlen, const int32_t *query_of, const int32_t *off,

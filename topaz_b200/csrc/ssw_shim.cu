@@ -11,10 +11,10 @@ extern "C" {
 }
 #include "search_internal.cuh"
 
-struct tpz_ssw_profile {
-    int8_t *read;        // as passed (init_destroy2 frees it)
-    int8_t *d_read;      // device copy
-    int32_t readLen;
+// the library-owned part of a profile: the matrix and the device copy of
+// the query
+struct tpz_ssw_device {
+    int8_t *d_read;
     int8_t mat[625];
 };
 
@@ -61,14 +61,22 @@ s_profile *ssw_init(const int8_t *read, const int32_t readLen, const int8_t *mat
         return nullptr;
     }
     s_profile *p = (s_profile *)calloc(1, sizeof(s_profile));
-    if (!p) return nullptr;
+    tpz_ssw_device *d = (tpz_ssw_device *)calloc(1, sizeof(tpz_ssw_device));
+    if (!p || !d) { free(p); free(d); return nullptr; }
     p->read = (int8_t *)read;
     p->readLen = readLen;
-    memcpy(p->mat, mat, 625);
-    if (cudaMalloc((void **)&p->d_read, readLen) != cudaSuccess ||
-        cudaMemcpy(p->d_read, read, readLen, cudaMemcpyHostToDevice) != cudaSuccess) {
+    p->n = n;
+    memcpy(d->mat, mat, 625);
+    int mn = 0;
+    for (int i = 0; i < 625; ++i) mn = std::min<int>(mn, mat[i]);
+    p->bias = (uint8_t)(-mn);
+    p->mat = d->mat;
+    p->device = d;
+    if (cudaMalloc((void **)&d->d_read, readLen) != cudaSuccess ||
+        cudaMemcpy(d->d_read, read, readLen, cudaMemcpyHostToDevice) != cudaSuccess) {
         tpz::cuda_fail(cudaGetLastError(), "ssw_init");
-        if (p->d_read) cudaFree(p->d_read);
+        if (d->d_read) cudaFree(d->d_read);
+        free(d);
         free(p);
         return nullptr;
     }
@@ -77,7 +85,10 @@ s_profile *ssw_init(const int8_t *read, const int32_t readLen, const int8_t *mat
 
 void init_destroy(s_profile *p) {
     if (!p) return;
-    if (p->d_read) cudaFree(p->d_read);
+    if (p->device) {
+        if (p->device->d_read) cudaFree(p->device->d_read);
+        free(p->device);
+    }
     free(p);
 }
 
@@ -106,11 +117,11 @@ s_align *ssw_align(const s_profile *prof, const int8_t *ref, int32_t refLen,
     }
     int rc;
     if (prof->readLen <= 1024) {
-        rc = tpz_sw_align_one(prof->d_read, prof->readLen, b->ref, refLen, prof->mat, weight_gapO,
-                              weight_gapE, b->meta + 2, st);
+        rc = tpz_sw_align_one(prof->device->d_read, prof->readLen, b->ref, refLen,
+                              prof->device->mat, weight_gapO, weight_gapE, b->meta + 2, st);
     } else {
-        rc = tpz::sw::batch_device_x(1, prof->d_read, b->offs, b->meta, b->ref, b->offs + 1,
-                                     b->meta + 1, prof->mat, weight_gapO, weight_gapE,
+        rc = tpz::sw::batch_device_x(1, prof->device->d_read, b->offs, b->meta, b->ref, b->offs + 1,
+                                     b->meta + 1, prof->device->mat, weight_gapO, weight_gapE,
                                      b->meta + 2, b->meta + 3, b->meta + 4, b->meta + 5, st,
                                      nullptr, nullptr, 0);
     }
@@ -144,7 +155,7 @@ int ssw_align_stats(const s_profile *prof, const int8_t *ref, int32_t refLen,
                     double *identity) {
     (void)maskLen;
     tpzh_stats s;
-    const int rc = tpzh_align_stats(prof->read, prof->readLen, ref, refLen, prof->mat, weight_gapO,
+    const int rc = tpzh_align_stats(prof->read, prof->readLen, ref, refLen, prof->device->mat, weight_gapO,
                                     weight_gapE, read_end1, ref_end1, score1, &s);
     *read_begin1 = s.qstart;
     *ref_begin1 = s.sstart;

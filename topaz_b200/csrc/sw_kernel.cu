@@ -52,8 +52,10 @@
 
 #include <algorithm>
 #include <mutex>
+#include <thread>
 #include <vector>
 
+#include "search_internal.cuh"
 #include "tpz_common.cuh"
 
 namespace tpz {
@@ -807,7 +809,7 @@ constexpr int kUsedRBins = kMaxR + kMaxStripes - 1;     // 39
 static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t *list,
                         const int32_t *list_n, int32_t *counts, int32_t *cursor, int32_t *sorted,
                         int32_t *multi_maxn, cudaStream_t st, int64_t &launches,
-                        int *host_maxn) {
+                        int *host_maxn, int known_maxn = -1) {
     const int nsm = sm_count();
     TPZ_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * kBins, st));
     const int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
@@ -821,8 +823,12 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
     if (host_maxn) {
         // the boundary buffer of multi-stripe bins is sized by the longest
         // subject among queries longer than one stripe
-        TPZ_CUDA(cudaMemcpyAsync(host_maxn, multi_maxn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-        TPZ_CUDA(cudaStreamSynchronize(st));
+        if (known_maxn >= 0) {
+            *host_maxn = known_maxn;
+        } else {
+            TPZ_CUDA(cudaMemcpyAsync(host_maxn, multi_maxn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            TPZ_CUDA(cudaStreamSynchronize(st));
+        }
         if (*host_maxn > 0) {
             a.bnd_words = 3 * ((int64_t)*host_maxn + 1);
             const size_t bytes = sizeof(uint32_t) * (size_t)a.bnd_words * nsm *
@@ -906,7 +912,7 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
-                   int score_only, const int32_t *subset, int64_t nsub) {
+                   int score_only, const int32_t *subset, int64_t nsub, int known_multi_maxn) {
     g_last_launches = 0;
     if (subset && nsub == 0) return TPZ_OK;
     if (n < 0 || n > INT32_MAX / 3 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
@@ -976,7 +982,7 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                           launches, &host_maxn);
     } else {
         rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, multi_maxn, st,
-                          launches, &host_maxn);
+                          launches, &host_maxn, known_multi_maxn);
     }
     if (rc) { if (a.bnd) cudaFreeAsync(a.bnd, st); cudaFreeAsync(ws, st); return rc; }
     a.ssw_lanes = 8;
@@ -1215,18 +1221,35 @@ int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t 
 
 namespace {
 
-// Grow-only device buffers reused by the host entry point.
+// Grow-only device buffers reused by the host entry point, and its streams:
+// one for the kernels, one for host-to-device and one for device-to-host
+// copies, so that a chunk's copies run beside another chunk's kernels.
 struct HostBatchBuffers {
     void *p = nullptr;
     size_t cap = 0;
     int dev = -1;
+    cudaStream_t compute = nullptr, h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev[8] = {};
 };
 thread_local HostBatchBuffers g_hb;
-thread_local cudaStream_t g_host_stream = nullptr;
 
 int ensure(size_t bytes) {
     int dev = 0;
     TPZ_CUDA(cudaGetDevice(&dev));
+    if (g_hb.compute && g_hb.dev != dev) {
+        // streams and events belong to the device they were made on
+        cudaStreamDestroy(g_hb.compute);
+        cudaStreamDestroy(g_hb.h2d);
+        cudaStreamDestroy(g_hb.d2h);
+        for (cudaEvent_t &e : g_hb.ev) { cudaEventDestroy(e); e = nullptr; }
+        g_hb.compute = g_hb.h2d = g_hb.d2h = nullptr;
+    }
+    if (!g_hb.compute) {
+        TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.compute, cudaStreamNonBlocking));
+        TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.h2d, cudaStreamNonBlocking));
+        TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.d2h, cudaStreamNonBlocking));
+        for (cudaEvent_t &e : g_hb.ev) TPZ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     if (g_hb.p && (g_hb.cap >= bytes) && g_hb.dev == dev) return TPZ_OK;
     if (g_hb.p) cudaFree(g_hb.p);
     g_hb.p = nullptr;
@@ -1234,8 +1257,35 @@ int ensure(size_t bytes) {
     TPZ_CUDA(cudaMalloc(&g_hb.p, bytes));
     g_hb.cap = bytes;
     g_hb.dev = dev;
-    if (!g_host_stream) TPZ_CUDA(cudaStreamCreateWithFlags(&g_host_stream, cudaStreamNonBlocking));
     return TPZ_OK;
+}
+
+// Residue byte ranges [lo, hi) of q and s that the pairs [i0, i1) read, and
+// the first pair outside the limits (-1: none).
+struct Span {
+    int64_t qlo, qhi, slo, shi, bad;
+    int multi_maxn;     // longest subject of a pair whose query spans several stripes
+};
+
+Span scan_pairs(int64_t i0, int64_t i1, const int64_t *qoff, const int32_t *qlen,
+                const int64_t *soff, const int32_t *slen) {
+    Span r{INT64_MAX, 0, INT64_MAX, 0, -1, 0};
+    for (int64_t i = i0; i < i1; ++i) {
+        if (qlen[i] < 1 || qlen[i] > TPZ_SW_MAX_QLEN || slen[i] < 0 || slen[i] >= TPZ_SW_MAX_SLEN ||
+            qoff[i] < 0 || soff[i] < 0) {
+            r.bad = i;
+            return r;
+        }
+        if (qlen[i] > tpz::sw::kStripeRows) r.multi_maxn = std::max(r.multi_maxn, slen[i]);
+        r.qlo = std::min(r.qlo, qoff[i]);
+        r.qhi = std::max(r.qhi, qoff[i] + qlen[i]);
+        if (slen[i] > 0) {
+            r.slo = std::min(r.slo, soff[i]);
+            r.shi = std::max(r.shi, soff[i] + slen[i]);
+        }
+    }
+    if (r.slo > r.shi) r.slo = r.shi;
+    return r;
 }
 
 }  // namespace
@@ -1308,19 +1358,38 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         return TPZ_E_ARG;
     }
     if (n == 0) return TPZ_OK;
-    // host-side validation: the residue spans must lie inside q / s
+    // Pairs go in up to three chunks of growing size (1/32, then up to 1/5,
+    // then the rest): the kernels of a chunk run while the residues of the
+    // next ones are copied in, and a chunk's results are copied out while
+    // later chunks compute, so only the first, small copy is not hidden.
+    int64_t cut[4] = {0, n, n, n};
+    int nch = 1;
+    if (n >= 65536) {
+        cut[1] = n / 32; cut[2] = n / 5; cut[3] = n;
+        nch = 3;
+    }
+    // host-side validation and the byte ranges each chunk reads, chunks
+    // scanned on their own threads
+    Span sp[3];
+    {
+        std::vector<std::thread> th;
+        for (int c = 1; c < nch; ++c)
+            th.emplace_back([&, c]() { sp[c] = scan_pairs(cut[c], cut[c + 1], qoff, qlen, soff, slen); });
+        sp[0] = scan_pairs(cut[0], cut[1], qoff, qlen, soff, slen);
+        for (auto &t : th) t.join();
+    }
     int64_t qbytes = 0, sbytes = 0;
-    for (int64_t i = 0; i < n; ++i) {
-        if (qlen[i] < 1 || qlen[i] > TPZ_SW_MAX_QLEN || slen[i] < 0 || slen[i] >= TPZ_SW_MAX_SLEN ||
-            qoff[i] < 0 || soff[i] < 0) {
+    for (int c = 0; c < nch; ++c) {
+        if (sp[c].bad >= 0) {
+            const int64_t i = sp[c].bad;
             char buf[160];
             snprintf(buf, sizeof buf, "tpz_sw_batch_host: pair %lld outside the limits (qlen %d, slen %d)",
                      (long long)i, qlen[i], slen[i]);
             tpz::set_error(buf);
             return TPZ_E_RANGE;
         }
-        qbytes = std::max(qbytes, qoff[i] + qlen[i]);
-        sbytes = std::max(sbytes, soff[i] + slen[i]);
+        qbytes = std::max(qbytes, sp[c].qhi);
+        sbytes = std::max(sbytes, sp[c].shi);
     }
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t bq = al(qbytes), bs = al(sbytes), b8 = al(8 * (size_t)n), b4 = al(4 * (size_t)n);
@@ -1338,21 +1407,62 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
     int32_t *dre = (int32_t *)d; d += b4;
     int32_t *drd = (int32_t *)d; d += b4;
     int32_t *dst = (int32_t *)d; d += b4;
-    cudaStream_t st = g_host_stream;
-    TPZ_CUDA(cudaMemcpyAsync(dq, q, qbytes, cudaMemcpyHostToDevice, st));
-    TPZ_CUDA(cudaMemcpyAsync(ds, s, sbytes, cudaMemcpyHostToDevice, st));
-    TPZ_CUDA(cudaMemcpyAsync(dqoff, qoff, 8 * n, cudaMemcpyHostToDevice, st));
-    TPZ_CUDA(cudaMemcpyAsync(dsoff, soff, 8 * n, cudaMemcpyHostToDevice, st));
-    TPZ_CUDA(cudaMemcpyAsync(dqlen, qlen, 4 * n, cudaMemcpyHostToDevice, st));
-    TPZ_CUDA(cudaMemcpyAsync(dslen, slen, 4 * n, cudaMemcpyHostToDevice, st));
-    rc = tpz::sw::batch_device(n, dq, dqoff, dqlen, ds, dsoff, dslen, mat625, gap_open, gap_extend,
-                               dsc, dre, drd, dst, st);
-    if (rc) return rc;
-    TPZ_CUDA(cudaMemcpyAsync(score, dsc, 4 * n, cudaMemcpyDeviceToHost, st));
-    TPZ_CUDA(cudaMemcpyAsync(ref_end, dre, 4 * n, cudaMemcpyDeviceToHost, st));
-    TPZ_CUDA(cudaMemcpyAsync(read_end, drd, 4 * n, cudaMemcpyDeviceToHost, st));
-    TPZ_CUDA(cudaMemcpyAsync(status, dst, 4 * n, cudaMemcpyDeviceToHost, st));
-    TPZ_CUDA(cudaStreamSynchronize(st));
+    cudaStream_t cs = g_hb.compute, hs = g_hb.h2d, os = g_hb.d2h;
+    // The device copies of q and s keep the host offsets.  Each chunk copies
+    // the part of its byte range not copied yet: the copied part is kept as
+    // one interval [lo, hi) that grows to cover every range seen (a gap
+    // between ranges is copied too, which is harmless).
+    int64_t qc_lo = 0, qc_hi = 0, sc_lo = 0, sc_hi = 0;
+    auto copy_new = [&](const int8_t *src, int8_t *dst, int64_t lo, int64_t hi, int64_t &c_lo,
+                        int64_t &c_hi) -> cudaError_t {
+        if (hi <= lo) return cudaSuccess;
+        if (c_hi <= c_lo) {
+            c_lo = lo; c_hi = hi;
+            return cudaMemcpyAsync(dst + lo, src + lo, hi - lo, cudaMemcpyHostToDevice, hs);
+        }
+        cudaError_t e = cudaSuccess;
+        if (lo < c_lo) {
+            e = cudaMemcpyAsync(dst + lo, src + lo, c_lo - lo, cudaMemcpyHostToDevice, hs);
+            c_lo = lo;
+        }
+        if (e == cudaSuccess && hi > c_hi) {
+            e = cudaMemcpyAsync(dst + c_hi, src + c_hi, hi - c_hi, cudaMemcpyHostToDevice, hs);
+            c_hi = hi;
+        }
+        return e;
+    };
+    cudaEvent_t *in_ready = g_hb.ev, *done = g_hb.ev + 3;
+    for (int c = 0; c < nch; ++c) {
+        const int64_t a = cut[c], m = cut[c + 1] - cut[c];
+        TPZ_CUDA(copy_new(q, dq, sp[c].qlo, sp[c].qhi, qc_lo, qc_hi));
+        TPZ_CUDA(copy_new(s, ds, sp[c].slo, sp[c].shi, sc_lo, sc_hi));
+        TPZ_CUDA(cudaMemcpyAsync(dqoff + a, qoff + a, 8 * m, cudaMemcpyHostToDevice, hs));
+        TPZ_CUDA(cudaMemcpyAsync(dsoff + a, soff + a, 8 * m, cudaMemcpyHostToDevice, hs));
+        TPZ_CUDA(cudaMemcpyAsync(dqlen + a, qlen + a, 4 * m, cudaMemcpyHostToDevice, hs));
+        TPZ_CUDA(cudaMemcpyAsync(dslen + a, slen + a, 4 * m, cudaMemcpyHostToDevice, hs));
+        TPZ_CUDA(cudaEventRecord(in_ready[c], hs));
+    }
+    for (int c = 0; c < nch; ++c) {
+        const int64_t a = cut[c], m = cut[c + 1] - cut[c];
+        TPZ_CUDA(cudaStreamWaitEvent(cs, in_ready[c], 0));
+        rc = tpz::sw::batch_device_x(m, dq, dqoff + a, dqlen + a, ds, dsoff + a, dslen + a,
+                                     mat625, gap_open, gap_extend, dsc + a, dre + a, drd + a,
+                                     dst + a, cs, nullptr, nullptr, 0, nullptr, 0,
+                                     sp[c].multi_maxn);
+        if (rc) {
+            cudaStreamSynchronize(hs);
+            cudaStreamSynchronize(cs);
+            return rc;
+        }
+        TPZ_CUDA(cudaEventRecord(done[c], cs));
+        TPZ_CUDA(cudaStreamWaitEvent(os, done[c], 0));
+        TPZ_CUDA(cudaMemcpyAsync(score + a, dsc + a, 4 * m, cudaMemcpyDeviceToHost, os));
+        TPZ_CUDA(cudaMemcpyAsync(ref_end + a, dre + a, 4 * m, cudaMemcpyDeviceToHost, os));
+        TPZ_CUDA(cudaMemcpyAsync(read_end + a, drd + a, 4 * m, cudaMemcpyDeviceToHost, os));
+        TPZ_CUDA(cudaMemcpyAsync(status + a, dst + a, 4 * m, cudaMemcpyDeviceToHost, os));
+    }
+    TPZ_CUDA(cudaStreamSynchronize(os));
+    TPZ_CUDA(cudaStreamSynchronize(cs));
     return TPZ_OK;
 }
 
@@ -1421,6 +1531,10 @@ namespace sw {
 
 constexpr int64_t kNoAllocMaxPairs = TPZ_SW_NOALLOC_MAX_PAIRS;
 constexpr int kNoAllocMaxQlen = TPZ_SW_NOALLOC_MAX_QLEN;   // one stripe
+// the stated entry limit is the largest one the 16-bit lanes hold exactly
+static_assert((int64_t)kNoAllocMaxQlen * TPZ_SW_NOALLOC_MAX_ENTRY < kBig &&
+                  (int64_t)kNoAllocMaxQlen * (TPZ_SW_NOALLOC_MAX_ENTRY + 1) >= kBig,
+              "TPZ_SW_NOALLOC_MAX_ENTRY");
 constexpr size_t kNoAllocWords = 2 * (size_t)kBins + 2 * kRBins + kRBins + 4 + 2 * (size_t)kNoAllocMaxPairs;
 
 // One copy per device that loads the library, kept until the process exits.
@@ -1519,6 +1633,25 @@ extern "C" int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int
         tpz::set_error("tpz_sw_batch_device_noalloc: NULL buffer");
         return TPZ_E_ARG;
     }
+    // 16-bit lanes are exact only while every score stays below the Fm
+    // reset addend and clear of the int16 limit; a query of up to
+    // kNoAllocMaxQlen rows can score at most kNoAllocMaxQlen * (largest
+    // entry).  The allocating call re-runs such pairs in 32 bits with
+    // scratch of its own; this one has none, so it refuses the matrix.
+    int mn = 0, mx = 0;
+    for (int i = 0; i < 625; ++i) {
+        mn = std::min<int>(mn, mat625_host[i]);
+        mx = std::max<int>(mx, mat625_host[i]);
+    }
+    if ((int64_t)kNoAllocMaxQlen * mx >= std::min(32767 - 2 * std::max(mx, 1), kBig)) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "tpz_sw_batch_device_noalloc: largest matrix entry %d is too large for exact "
+                 "16-bit scores of %d-residue queries (limit %d); use tpz_sw_batch_device",
+                 mx, kNoAllocMaxQlen, TPZ_SW_NOALLOC_MAX_ENTRY);
+        tpz::set_error(buf);
+        return TPZ_E_ARG;
+    }
     const NoAllocDev *d = nullptr;
     int rc = noalloc_setup(&d);
     if (rc) return rc;
@@ -1537,8 +1670,6 @@ extern "C" int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int
     a.sorted = sorted; a.rinfo = rinfo; a.next_task = next_task;
     a.rerun = rerun; a.rerun_count = rerun_count;
     a.gap_open = gap_open; a.gap_extend = gap_extend;
-    int mn = 0;
-    for (int i = 0; i < 625; ++i) mn = std::min<int>(mn, mat625_host[i]);
     a.bias = -mn;
     memcpy(a.mat, mat625_host, 625);
     a.translate = 0;

@@ -67,9 +67,11 @@ static int map_file(const char *prefix, const char *ext, map_t *m) {
     struct stat sb;
     if (fd < 0 || fstat(fd, &sb) != 0) return -1;
     m->size = (uint64_t)sb.st_size;
-    m->data = m->size ? mmap(NULL, m->size, PROT_READ, MAP_PRIVATE, fd, 0) : NULL;
+    /* an empty file fails here with EINVAL, as fmmap_ro's mmap does
+     * (src/utils.c:17-42) */
+    m->data = mmap(NULL, m->size, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (m->data == MAP_FAILED) return -1;
     close(fd);
-    if (m->size && m->data == MAP_FAILED) return -1;
     return 0;
 }
 
@@ -342,31 +344,38 @@ static void *search_worker(void *arg) {
 int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     struct timeval t0, t1;
     gettimeofday(&t0, NULL);
+    /* db_load / _load_index (src/db.c:34-122) in the same order, with the
+     * same messages; a file that cannot be mapped ends the process with
+     * engine_init's message (src/engine.c:47-50) */
     map_t T, SA, phr, ind;
-    if (map_file(prefix, ".psq", &T) || map_file(prefix, ".SA", &SA) || map_file(prefix, ".phr", &phr)) {
-        fprintf(stderr, "Error: could not load database, %s\n", strerror(errno));
-        return -1;
-    }
+    if (map_file(prefix, ".psq", &T)) goto load_fail;
     fprintf(stderr, "read T (%s.psq), file size is %" PRIu64 " bytes\n", prefix, T.size);
+    if (map_file(prefix, ".SA", &SA)) goto load_fail;
     fprintf(stderr, "read SA (%s.SA), file size is %" PRIu64 " bytes\n", prefix, SA.size);
     if (SA.size != T.size * 8) {
         fprintf(stderr, "Error: SA (%s.SA, %" PRIu64 " bytes) should be 8 x T (%s.psq, %" PRIu64 " bytes)!\nExiting...\n",
                 prefix, SA.size, prefix, T.size);
         exit(EXIT_FAILURE);
     }
+    if (map_file(prefix, ".phr", &phr)) goto load_fail;
+    fprintf(stderr, "read protein headers (%s.phr), file size is %" PRIu64 " bytes\n", prefix, phr.size);
     uint64_t Psize = 0;
     for (uint64_t i = 0; i < phr.size; ++i) {
         if (phr.data[i] == '\0') break;
         if (phr.data[i] == '\n') Psize++;
     }
-    fprintf(stderr, "read protein headers (%s.phr), file size is %" PRIu64 " bytes\n", prefix, phr.size);
     fprintf(stderr, "%" PRIu64 " proteins in database\n", Psize);
     if (map_file(prefix, ".ind", &ind)) {
         fprintf(stderr, "Error: could not open %s.ind, %s\n", prefix, strerror(errno));
-        return -1;
+        goto load_fail;
     }
     if (ind.size != Psize * 24) {
         fprintf(stderr, "Error: index is the wrong size (read %" PRIu64 ", expected %" PRIu64 ")", ind.size, Psize * 24);
+        exit(EXIT_FAILURE);
+    }
+    if (0) {
+load_fail:
+        fprintf(stderr, "Error: could not load database, %s\n", strerror(errno));
         exit(EXIT_FAILURE);
     }
     const uint64_t db_size = T.size - Psize, db_proteins = Psize;
