@@ -260,12 +260,27 @@ TPZ_API int tpz_prepare_queries(char *cat, const int64_t *off, const int32_t *le
                                 int seg, int nthreads);
 
 /* Suffix array of the .psq bytes T[0, n) on the device, for `topaz index`
- * (serif_index / create_index, src/index.c:24-93, build it on the host):
+ * (divsufsort64 in serif_index, src/index.c:24-93, builds it on the host):
  * SA[0, n) (host) receives the suffixes in byte-lexicographic order, a
  * shorter suffix before a longer one with the same prefix -- the bytes of the
  * reference's .SA file.  rounds (may be NULL) receives the number of sorting
- * rounds.  n must be below 2^32 - 1 (TPZ_E_RANGE otherwise). */
+ * rounds.  64-bit positions; the text, its inverse array (8 bytes per
+ * position) and the sort buffers must fit in device memory (about 10 G
+ * residues on one B200); TPZ_E_RANGE for texts where more suffixes share
+ * their first few symbols than one device sort holds. */
 TPZ_API int tpz_sa_build(const uint8_t *T, int64_t n, int64_t *SA, int32_t *rounds);
+
+/* The same with the rows handed to a sink instead of one host array, so the
+ * caller never holds the whole array (8 bytes per text byte) in memory:
+ * sink(user, first_row, rows, count) receives SA[first_row .. first_row +
+ * count); rows come mostly in increasing order, and rows inside long repeats
+ * come again at the end with their final values (a file sink writes each
+ * piece at its offset).  A nonzero return from the sink stops the build
+ * (TPZ_E_ARG).  max_partition > 0 caps the suffixes sorted at once (0: as
+ * the free device memory allows). */
+typedef int (*tpz_sa_sink)(void *user, int64_t first_row, const int64_t *rows, int64_t count);
+TPZ_API int tpz_sa_build_sink(const uint8_t *T, int64_t n, tpz_sa_sink sink, void *user,
+                              int64_t max_partition, int32_t *rounds);
 
 /* bitscore and E-value of a raw score exactly as align_using_ssw_profile
  * computes them with the C library's log/exp (src/ssw_wrapper.c:179-183,

@@ -9,7 +9,6 @@ import numpy as np
 import pytest
 
 import oracle
-from sa_util import suffix_array
 from topaz_b200 import build as B, native, synth
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -19,7 +18,6 @@ needs_ref = pytest.mark.skipif(oracle.libref() is None, reason="oracle/_ref not 
 def host():
     L = native.lib()
     L.tpzh_seg_mask.argtypes = [ctypes.c_char_p, ctypes.c_int]
-    L.tpzh_suffix_array.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
     return L
 
 
@@ -89,22 +87,6 @@ def test_seg_matches_live_reference():
         assert a.raw[:len(s)] == b.raw[:len(s)]
 
 
-def test_suffix_array_sais():
-    L = host()
-    for seed, n in ((1, 50), (2, 400), (3, 2000)):
-        prot = synth.protein_db(n, seed=seed)
-        from topaz_b200 import dbformat
-        db = dbformat.build_from_records([(p.encode(), s) for p, s in zip(prot.ids, prot.seqs)])
-        sa = np.zeros(db.Tsize, np.int64)
-        assert L.tpzh_suffix_array(db.T.ctypes.data, db.Tsize, sa.ctypes.data) == 0
-        assert (sa == suffix_array(db.T)).all()
-    for t in (b"\n", b"A\n", b"AAAAAAAAAA\n", b"ABABABAB\nAB\n", b"YXYXYX\n\n\nA\n"):
-        T = np.frombuffer(t, np.uint8).copy()
-        sa = np.zeros(len(T), np.int64)
-        assert L.tpzh_suffix_array(T.ctypes.data, len(T), sa.ctypes.data) == 0
-        assert (sa == suffix_array(T)).all()
-
-
 def _fasta_cases(tmp):
     prot = synth.protein_db(120, seed=4)
     path = os.path.join(tmp, "db.fa")
@@ -116,7 +98,9 @@ def _fasta_cases(tmp):
 
 
 @needs_ref
-def test_index_files_match_reference(tmp_path):
+@pytest.mark.gpu
+def test_index_files_match_reference(cuda, tmp_path):
+    # `topaz index` builds the suffix array on the device
     B.build()
     for fa in _fasta_cases(str(tmp_path)):
         outs = {}

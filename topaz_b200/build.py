@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["tpz_common.cu", "sw_kernel.cu", "search_kernels.cu", "search_host.cu", "sa_build.cu", "ssw_shim.cu"]
 HOSTDIR = os.path.join(HERE, "host")
-HOST_SOURCES = ["tpzh_fasta.c", "tpzh_seg.c", "tpzh_sais.c", "tpzh_index.c", "tpzh_stats.c",
+HOST_SOURCES = ["tpzh_fasta.c", "tpzh_seg.c", "tpzh_index.c", "tpzh_stats.c",
                 "tpzh_search.c", "tpzh_main.c", "tpzh_prepare.c"]
 CLI = os.path.join(LIBDIR, "topaz")
 CC = os.environ.get("CC", "gcc")

@@ -52,8 +52,6 @@ TPZH_API int tpzh_header_id(const char *buf, int len, const char **id);
 TPZH_API int tpzh_seg_mask(char *seq, int len);
 
 /* ---------------------------------------------------------------- index */
-/* suffix array of T[0, n) (byte order, shorter suffix first) */
-TPZH_API int tpzh_suffix_array(const uint8_t *T, int64_t n, int64_t *SA);
 /* `topaz index -f FASTA -p PREFIX` (serif_index, src/index.c:24-93) */
 TPZH_API int tpzh_index(const char *fasta, const char *prefix);
 

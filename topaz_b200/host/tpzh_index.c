@@ -15,6 +15,7 @@
 #include "../../include/topaz_b200.h"
 
 #include <errno.h>
+#include <fcntl.h>
 #include <inttypes.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -41,6 +42,26 @@ typedef struct {
     uint64_t header_start, protein_start;
     int32_t header_len, protein_len;
 } ind_rec;
+
+typedef struct {
+    int fd;
+    int err;     /* errno of a failed write */
+} sa_file_t;
+
+/* tpz_sa_build_sink's sink: rows [first_row, first_row + count) at their
+ * offset in the .SA file */
+static int sa_to_file(void *user, int64_t first_row, const int64_t *rows, int64_t count) {
+    sa_file_t *f = (sa_file_t *)user;
+    const char *p = (const char *)rows;
+    size_t left = (size_t)count * 8;
+    off_t at = (off_t)first_row * 8;
+    while (left > 0) {
+        const ssize_t w = pwrite(f->fd, p, left, at);
+        if (w <= 0) { f->err = errno ? errno : EIO; return -1; }
+        p += w; at += w; left -= (size_t)w;
+    }
+    return 0;
+}
 
 int tpzh_index(const char *fasta, const char *prefix) {
     /* ---- demultiplex */
@@ -76,24 +97,23 @@ int tpzh_index(const char *fasta, const char *prefix) {
     fclose(tf);
     fprintf(stderr, "mmapped T (%s), file size is %" PRId64 " bytes\n", tn, Tsize);
     free(tn);
-    int64_t *SA = malloc(sizeof(int64_t) * (Tsize > 0 ? Tsize : 1));
-    if (!SA) { fprintf(stderr, "suffix array construction failed\n"); return -1; }
-    /* on the GPU (prefix doubling); the host SA-IS when there is none or
-     * the text is too long for it -- both give the same array */
-    if (tpz_sa_build(T, Tsize, SA, NULL) != 0) {
-        fprintf(stderr, "GPU suffix array unavailable (%s); building it on the host\n", tpz_last_error());
-        if (tpzh_suffix_array(T, Tsize, SA) != 0) {
-            fprintf(stderr, "suffix array construction failed\n");
-            return -1;
-        }
+    /* on the GPU, streamed into the .SA file piece by piece (the whole
+     * array, 8 bytes per text byte, is never held in host memory) */
+    char *san = fname(prefix, ".SA");
+    const int safd = open(san, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (safd < 0) { fprintf(stderr, "Error: could not open %s, %s\n", san, strerror(errno)); return -1; }
+    if (ftruncate(safd, Tsize * 8) != 0) { fprintf(stderr, "Error: could not size %s, %s\n", san, strerror(errno)); return -1; }
+    sa_file_t out = {safd, 0};
+    if (tpz_sa_build_sink(T, Tsize, sa_to_file, &out, 0, NULL) != 0) {
+        fprintf(stderr, "Error: suffix array construction failed (%s)\n",
+                out.err ? strerror(out.err) : tpz_last_error());
+        return -1;
     }
-    FILE *sa = open_w(prefix, ".SA");
-    if (!sa || fwrite(SA, sizeof(int64_t), Tsize, sa) != (size_t)Tsize) return -1;
-    fclose(sa);
+    if (close(safd) != 0) { fprintf(stderr, "Error: could not write %s\n", san); return -1; }
+    free(san);
     FILE *isa = open_w(prefix, ".ISA");
     if (!isa || ftruncate(fileno(isa), Tsize * 8) != 0) return -1;
     fclose(isa);
-    free(SA);
     free(T);
 
     /* ---- .ind from .pin */

@@ -272,15 +272,17 @@ def protein_db_arrays(n: int, seed: int = 0, median=300, lo=50, hi=2000):
     return random_residues(rng, int(lens.sum())), lens
 
 
-def search_queries_arrays(res: np.ndarray, lens: np.ndarray, n_mut: int, n_rand: int,
+def search_queries_arrays(res, lens: np.ndarray, n_mut: int, n_rand: int,
                           seed: int = 2, identity=(0.30, 0.90), lo=50, hi=1500):
     """Queries for the full-search configs: n_mut mutated from random DB
     proteins (identity uniform in `identity`, indels at 0.02), n_rand random,
-    lengths clipped to [lo, hi].  Returns (residues, lengths)."""
+    lengths clipped to [lo, hi].  `res` is the DB's concatenated residues, or
+    a function giving the concatenated residues of a list of protein
+    numbers.  Returns (residues, lengths)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     off = np.cumsum(lens) - lens
     pick = rng.integers(0, len(lens), n_mut)
-    src = res[_segment_positions(off[pick], lens[pick])]
+    src = res(pick) if callable(res) else res[_segment_positions(off[pick], lens[pick])]
     mres, mlen = mutate_batch(rng, src, lens[pick], rng.uniform(*identity, size=n_mut))
     rlen = lognormal_lengths(rng, n_rand, 300, lo, hi)
     rres = random_residues(rng, int(rlen.sum()))
@@ -296,3 +298,74 @@ def search_queries_arrays(res: np.ndarray, lens: np.ndarray, n_mut: int, n_rand:
         plens.append(len(s))
     allres = np.concatenate(parts + [rres])
     return allres, np.concatenate([np.array(plens, np.int64), rlen])
+
+
+FASTA_ID_DIGITS = 9
+
+
+def _db_fasta_chunk(args):
+    """Worker: one chunk of records of write_db_fasta, written at its offset."""
+    path, seed, k, a, lens, rec_off, prefix = args
+    lens = np.asarray(lens, dtype=np.int64)
+    pre = (">" + prefix).encode()
+    hw = len(pre) + FASTA_ID_DIGITS + 1
+    rec = hw + lens + 1
+    start = np.concatenate([[0], np.cumsum(rec)[:-1]])
+    rng = np.random.Generator(np.random.PCG64([seed, k]))
+    # residues drawn for every byte of the chunk; the header and newline
+    # bytes are then written over them, so each sequence stays i.i.d.
+    buf = random_residues(rng, int(rec.sum()))
+    for j, c in enumerate(pre):
+        buf[start + j] = c
+    num = np.arange(a, a + len(lens), dtype=np.int64)
+    for j in range(FASTA_ID_DIGITS):
+        buf[start + len(pre) + FASTA_ID_DIGITS - 1 - j] = ord("0") + (num // 10 ** j) % 10
+    buf[start + hw - 1] = ord("\n")
+    buf[start + hw + lens] = ord("\n")
+    fd = os.open(path, os.O_WRONLY)
+    try:
+        mv = memoryview(buf)
+        done = 0
+        while done < len(buf):
+            done += os.pwrite(fd, mv[done:], rec_off + done)
+    finally:
+        os.close(fd)
+    return len(buf)
+
+
+def write_db_fasta(path: str, n: int, seed: int = 0, median=300, lo=50, hi=2000,
+                   id_prefix: str = "db", chunk: int = 1_000_000, workers: int = 0):
+    """An n-protein DB with the lengths and residue model of protein_db_arrays
+    written straight to FASTA (IDs id_prefix + 9 digits, one sequence line
+    per record), chunk by chunk in `workers` processes -- for DBs of 10^7 to
+    10^8 proteins that should not sit in memory twice.  Returns (lens,
+    seq_start): the sequence lengths and the file offset of each sequence,
+    so that callers can read proteins back from the file."""
+    import multiprocessing as mp
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lens = lognormal_lengths(rng, n, median, lo, hi)
+    hw = len(id_prefix) + 2 + FASTA_ID_DIGITS
+    rec = hw + lens + 1
+    rec_start = np.concatenate([[0], np.cumsum(rec)[:-1]])
+    total = int(rec.sum())
+    with open(path, "wb") as f:
+        f.truncate(total)
+    jobs = [(path, seed, k, a, lens[a:a + chunk], int(rec_start[a]), id_prefix)
+            for k, a in enumerate(range(0, n, chunk))]
+    workers = workers or min(len(jobs), os.cpu_count() or 1)
+    if workers <= 1:
+        for j in jobs:
+            _db_fasta_chunk(j)
+    else:
+        with mp.get_context("spawn").Pool(workers) as pool:
+            pool.map(_db_fasta_chunk, jobs)
+    return lens, rec_start + hw
+
+
+def fasta_residues(mm, seq_start: np.ndarray, lens: np.ndarray, pick) -> np.ndarray:
+    """Residues of records `pick` of a FASTA written by write_db_fasta
+    (mm: its bytes, e.g. an np.memmap), concatenated."""
+    if len(pick) == 0:
+        return np.zeros(0, np.uint8)
+    return np.concatenate([np.asarray(mm[seq_start[i]:seq_start[i] + lens[i]]) for i in pick])
+
