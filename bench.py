@@ -63,6 +63,15 @@ def parse():
                          "equal share per worker thread (mid size), 2500 (large)")
     ap.add_argument("--no-search", action="store_true",
                     help="skip the full-search (config 2) section")
+    ap.add_argument("--config3", action="store_true",
+                    help="run only the large full search (30M proteins, 10^5 queries) through the "
+                         "topaz CLI against the reference binary and print its JSON")
+    ap.add_argument("--c3-proteins", type=int, default=30_000_000)
+    ap.add_argument("--c3-queries", type=int, default=100_000)
+    ap.add_argument("--c3-dir", default="/dev/shm/tpz_c3",
+                    help="working directory of --config3 (DB files: ~10.5 bytes per residue)")
+    ap.add_argument("--c3-ref-seconds", type=float, default=30.0,
+                    help="reference run time per mode on its query sample")
     return ap.parse_args()
 
 
@@ -499,6 +508,126 @@ def search_bench(args, dev):
     return out
 
 
+C3_WORKLOAD = ("full search, large: %d-protein synthetic DB (log-normal lengths median 300, "
+               "50-2000, Robinson-Robinson residues; %.2f G residues, int64 SA %.1f GB), %d queries "
+               "of 50-1500 residues (half mutated from DB proteins at 30-90%% identity with "
+               "indels, half random), SEG on, BLOSUM62 11/1, -H 100 -E 1e-3; default, --fast "
+               "and --blasttab")
+
+
+def config3_bench(args):
+    """The large full search end to end through the command line: the DB
+    FASTA is written, `topaz index` (ours; suffix array on the device) builds
+    the files, our `topaz search` runs all queries in default, --fast and
+    --blasttab modes, and the reference binary `topaz search -T nproc` runs
+    an evenly spaced query sample of each mode on the same files; outputs
+    are compared per query block."""
+    import shutil
+
+    import oracle
+    from topaz_b200 import build as B, synth
+    threads = os.cpu_count() or 1
+    d = args.c3_dir
+    shutil.rmtree(d, ignore_errors=True)
+    os.makedirs(d)
+    out = {}
+    try:
+        fa, qfa, pre = os.path.join(d, "db.fa"), os.path.join(d, "q.fa"), os.path.join(d, "db")
+        t0 = time.perf_counter()
+        lens, sstart = synth.write_db_fasta(fa, args.c3_proteins, seed=args.seed + 41)
+        residues = int(lens.sum())
+        need = int(11.5 * residues)
+        free = shutil.disk_usage(d).free
+        if free < need:
+            return {"unavailable": "working directory %s has %.0f GB free, the DB needs ~%.0f GB"
+                                   % (d, free / 1e9, need / 1e9)}
+        mm = np.memmap(fa, np.uint8, mode="r")
+        nq = args.c3_queries
+        qres, qlens = synth.search_queries_arrays(
+            lambda pick: synth.fasta_residues(mm, sstart, lens, pick), lens, nq // 2, nq - nq // 2,
+            seed=args.seed + 42)
+        del mm
+        qoff = np.cumsum(qlens) - qlens
+        ids = ["q%d" % i for i in range(nq)]
+        synth.write_fasta(qfa, synth.Proteins(ids, [qres[o:o + n] for o, n in zip(qoff, qlens)]))
+        gen_s = time.perf_counter() - t0
+        out["workload"] = C3_WORKLOAD % (args.c3_proteins, residues / 1e9, 8 * (residues + len(lens)) / 1e9, nq)
+        out["generate_s"] = round(gen_s, 1)
+        # `topaz index` (ours): FASTA -> .pin/.psq/.phr/.ind, SA on the device
+        t0 = time.perf_counter()
+        r = subprocess.run([B.CLI, "index", "-f", fa, "-p", pre], capture_output=True)
+        out["index"] = {"seconds": round(time.perf_counter() - t0, 1), "rc": r.returncode,
+                        "stderr_tail": r.stderr.decode(errors="replace")[-400:],
+                        "sa_bytes": os.path.getsize(pre + ".SA") if os.path.exists(pre + ".SA") else 0}
+        os.remove(fa)
+        if r.returncode != 0:
+            return out
+
+        def run(exe, qpath, extra, dst):
+            with open(dst, "wb") as fo:
+                t = time.perf_counter()
+                rr = subprocess.run([exe, "search", "-f", qpath, "-p", pre, "-T", str(threads), *extra],
+                                    stdout=fo, stderr=subprocess.PIPE, cwd=d)
+                return time.perf_counter() - t, rr
+
+        def blocks(path, keep=None):
+            bl = {}
+            with open(path, "rb") as fh:
+                head = fh.readline()
+                for ln in fh:
+                    q = ln.split(b"\t", 1)[0]
+                    if keep is None or q in keep:
+                        bl.setdefault(q, []).append(ln)
+            return head, bl
+
+        def spread(n):
+            return np.unique(np.linspace(0, nq - 1, n).astype(np.int64)).tolist()
+
+        modes = (("default", []), ("fast", ["--fast"]), ("blasttab", ["--blasttab"]))
+        for mode, extra in modes:
+            dst = os.path.join(d, "ours_%s.out" % mode)
+            dt, rr = run(B.CLI, qfa, extra, dst)
+            timing = [ln for ln in rr.stderr.decode(errors="replace").splitlines()
+                      if ln.startswith("timing:")]
+            out[mode] = {"queries_per_s": round(nq / dt, 1), "wall_s": round(dt, 1),
+                         "rc": rr.returncode, "stages": timing[0] if timing else None,
+                         "api": "topaz search CLI, whole process, -T %d" % threads}
+        if not os.path.exists(oracle.REF_BIN):
+            return out
+        # the reference on evenly spaced samples (mutated and random halves)
+        probe = spread(2 * threads)
+        pf = os.path.join(d, "probe.fa")
+        synth.write_fasta(pf, synth.Proteins([ids[i] for i in probe],
+                                             [qres[qoff[i]:qoff[i] + qlens[i]] for i in probe]))
+        dt, _ = run(oracle.REF_BIN, pf, [], os.path.join(d, "probe.out"))
+        rate = len(probe) / dt
+        for mode, extra in modes:
+            n = int(min(nq, max(2 * threads, rate * args.c3_ref_seconds * (2.0 if mode == "fast" else 1.0))))
+            sample = spread(n)
+            sf = os.path.join(d, "sample_%s.fa" % mode)
+            synth.write_fasta(sf, synth.Proteins([ids[i] for i in sample],
+                                                 [qres[qoff[i]:qoff[i] + qlens[i]] for i in sample]))
+            dst = os.path.join(d, "ref_%s.out" % mode)
+            dr, rr = run(oracle.REF_BIN, sf, extra, dst)
+            keep = {ids[i].encode() for i in sample}
+            h1, b1 = blocks(dst)
+            h2, b2 = blocks(os.path.join(d, "ours_%s.out" % mode), keep)
+            ref_qps = len(sample) / dr
+            out[mode].update({
+                "reference_queries_per_s": round(ref_qps, 2),
+                "reference_sample": "%d queries evenly spaced over the %d (%d mutated, %d random), "
+                                    "topaz search -T %d" % (len(sample), nq,
+                                                            sum(i < nq // 2 for i in sample),
+                                                            sum(i >= nq // 2 for i in sample), threads),
+                "reference_rc": rr.returncode,
+                "over_reference": round(out[mode]["queries_per_s"] / ref_qps, 1),
+                "identical_blocks": h1 == h2 and b1 == b2,
+                "blocks_compared": len(b1), "lines_compared": sum(len(v) for v in b1.values())})
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def per_pair_bench(torch, t, ps, mat, dev, batched_gcups, npairs=20000, nstreams=(1, 16)):
     """GCUPS of one kernel launch per pair (tpz_sw_align_one) on an evenly
     spaced sample of the workload's pairs with qlen <= 1024, launched from
@@ -742,7 +871,9 @@ def main():
     rank, local_rank, world = dist_env()
     if args.warmup < 3 and args.impl == "native":
         args.warmup = 3
-    if args.impl == "reference":
+    if args.config3:
+        line = {"search_config3": config3_bench(args)} if rank == 0 else None
+    elif args.impl == "reference":
         line = reference_arm(args, rank, world)
     else:
         line = native_arm(args, rank, local_rank, world)

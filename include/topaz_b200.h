@@ -129,6 +129,24 @@ TPZ_API int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int64_
                                         int32_t *ref_end, int32_t *read_end, int32_t *status,
                                         void *stream);
 
+/* The --blasttab columns of n aligned pairs on the device: what
+ * ssw_align_stats (src/ssw.c:900-978) computes for a hit whose forward pass
+ * gave (score, read_end, ref_end) -- query and subject starts from a reverse
+ * pass, then length, gap opens, mismatches and identity from the banded
+ * alignment's path (src/ssw.c:538-784).  Pairs as tpz_sw_batch_device
+ * (device buffers, matrix-index residues); read_end/ref_end/score per pair;
+ * outputs per pair; -1 columns (identity -1.0) where the reference gives
+ * them (no end cell, no start found, the band table's size guard).  Work
+ * goes on `stream`; the call waits for it (it sizes scratch from the
+ * device's results). */
+TPZ_API int tpz_sw_stats_device(int64_t n, const int8_t *q, const int64_t *qoff,
+                                const int32_t *qlen, const int8_t *s, const int64_t *soff,
+                                const int32_t *slen, const int8_t *mat625_host, int gap_open,
+                                int gap_extend, const int32_t *read_end, const int32_t *ref_end,
+                                const int32_t *score, int32_t *qstart, int32_t *sstart,
+                                int32_t *length, int32_t *gapopen, int32_t *mismatch,
+                                double *identity, void *stream);
+
 /* Kernel launches enqueued by the last tpz_sw_batch_* call on this thread
  * (for launch accounting). */
 TPZ_API int64_t tpz_sw_last_launches(void);
@@ -224,6 +242,9 @@ typedef struct {
     double max_evalue;        /* -E */
     double lambda, k, H;      /* Karlin-Altschul parameters (0.267, 0.041, 0.140) */
     uint64_t db_size, db_proteins;
+    /* report mode only: 1 = also the --blasttab columns of every reported
+     * hit on the device (ssw_align_stats, src/ssw.c:900-978) */
+    int32_t blasttab_stats;
 } tpz_search_opts;
 
 typedef struct {
@@ -243,6 +264,11 @@ typedef struct {
     int64_t sw_pairs, sw_cells;              /* SW of hits: pairs, sum of qlen * slen */
     double seed_ms, chain_ms;                /* stage_ms[0] split: seed lookup, cursor chains */
     int64_t positions;                       /* query positions searched */
+    /* per reported hit when opts.blasttab_stats (else NULL): 0-based query
+     * and subject starts, alignment length, gap opens, mismatches, identity;
+     * -1 columns for hits without a Smith-Waterman alignment */
+    const int32_t *qstart, *sstart, *length, *gapopen, *mismatch;
+    const double *identity;
 } tpz_search_result;
 
 TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,

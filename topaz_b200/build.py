@@ -18,7 +18,8 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libtopaz_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["tpz_common.cu", "sw_kernel.cu", "search_kernels.cu", "search_host.cu", "sa_build.cu", "ssw_shim.cu"]
+SOURCES = ["tpz_common.cu", "sw_kernel.cu", "search_kernels.cu", "search_host.cu", "sa_build.cu", "ssw_shim.cu",
+           "stats_kernel.cu"]
 HOSTDIR = os.path.join(HERE, "host")
 HOST_SOURCES = ["tpzh_fasta.c", "tpzh_seg.c", "tpzh_index.c", "tpzh_stats.c",
                 "tpzh_search.c", "tpzh_main.c", "tpzh_prepare.c"]

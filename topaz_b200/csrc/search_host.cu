@@ -398,6 +398,8 @@ struct ResultHolder {
     std::vector<int32_t> status, protein, gs, gl, so, raw, qend, send, sw_status;
     std::vector<int32_t> trace_off, trace_score, trace_len, trace_counted;
     std::vector<double> bits, evalue;
+    std::vector<int32_t> st_qstart, st_sstart, st_length, st_gapopen, st_mismatch;
+    std::vector<double> st_identity;
     int64_t sw_pairs = 0, sw_cells = 0;
 };
 
@@ -474,6 +476,8 @@ struct HitPairs {                 // the SW pairs of a batch and where they came
     const int64_t *pq_off, *ps_off;
     const int32_t *pq_len, *ps_len, *hit2pair;
     const int8_t *xmap;           // host, 128 entries
+    const int64_t *qoff_q;        // device: text offset of each query
+    const int64_t *pstart;        // device: text offset of each protein
 };
 
 int report_select(DevBuf &b, ResultHolder *R, int64_t nq, int64_t maxq, const int32_t *qlen,
@@ -553,6 +557,30 @@ int report_select(DevBuf &b, ResultHolder *R, int64_t nq, int64_t maxq, const in
     for (int f = 0; f < kGatherFields; ++f) {
         host[f]->resize(n);
         if (n) TPZ_CUDA(cudaMemcpy(host[f]->data(), dst[f], 4 * n, cudaMemcpyDeviceToHost));
+    }
+    if (o->blasttab_stats && n > 0) {
+        // the --blasttab columns of the reported hits, on the device
+        std::vector<int32_t> qof(n);
+        for (int64_t q = 0; q < nq; ++q)
+            for (int64_t h = R->hit_off[q]; h < R->hit_off[q + 1]; ++h) qof[h] = (int32_t)q;
+        int32_t *d_qof, *sto[5];
+        double *d_id;
+        if ((rc = b.alloc(&d_qof, n)) || (rc = b.alloc(&d_id, n))) return rc;
+        for (int f = 0; f < 5; ++f)
+            if ((rc = b.alloc(&sto[f], n))) return rc;
+        TPZ_CUDA(cudaMemcpy(d_qof, qof.data(), 4 * n, cudaMemcpyHostToDevice));
+        rc = tpz::stats::reported_stats(n, hp.q, hp.qoff_q, d_qof, hp.T, hp.pstart, dst[0], dst[4],
+                                        dst[5], dst[6], dst[7], o->mat625, hp.xmap, o->gap_open,
+                                        o->gap_extend, sto[0], sto[1], sto[2], sto[3], sto[4], d_id, 0);
+        if (rc) return rc;
+        std::vector<int32_t> *sh[5] = {&R->st_qstart, &R->st_sstart, &R->st_length, &R->st_gapopen,
+                                       &R->st_mismatch};
+        for (int f = 0; f < 5; ++f) {
+            sh[f]->resize(n);
+            TPZ_CUDA(cudaMemcpy(sh[f]->data(), sto[f], 4 * n, cudaMemcpyDeviceToHost));
+        }
+        R->st_identity.resize(n);
+        TPZ_CUDA(cudaMemcpy(R->st_identity.data(), d_id, 8 * n, cudaMemcpyDeviceToHost));
     }
     R->bits.resize(n);
     R->evalue.resize(n);
@@ -973,6 +1001,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
             hp.q = (const int8_t *)dq; hp.T = (const int8_t *)ix->d.T; hp.pq_off = pq_off;
             hp.ps_off = ps_off; hp.pq_len = pq_len; hp.ps_len = ps_len;
             hp.hit2pair = npairs > 0 ? hit2pair : nullptr; hp.xmap = xmap;
+            hp.qoff_q = dqo; hp.pstart = ix->d.pstart;
             int rc2 = report_select(b, R, nq, maxq, qlen, o, rt, nh, pprot, pgs, pgl, pso, raw, qend, send,
                                     psw, hp, ev[3]);
             if (rc2) return bail(rc2);
@@ -1021,6 +1050,15 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         r.nhits_total = R->hit_off[nq];
         r.bitscore = R->bits.data();
         r.evalue = R->evalue.data();
+        if (o->blasttab_stats) {
+            // every reported hit has its columns (none when nothing was reported)
+            const int64_t n = R->hit_off[nq];
+            R->st_qstart.resize(n); R->st_sstart.resize(n); R->st_length.resize(n);
+            R->st_gapopen.resize(n); R->st_mismatch.resize(n); R->st_identity.resize(n);
+            r.qstart = R->st_qstart.data(); r.sstart = R->st_sstart.data();
+            r.length = R->st_length.data(); r.gapopen = R->st_gapopen.data();
+            r.mismatch = R->st_mismatch.data(); r.identity = R->st_identity.data();
+        }
     }
     TPZ_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
     float t01 = 0, t12 = 0, t23 = 0;

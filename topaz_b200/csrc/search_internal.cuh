@@ -123,4 +123,18 @@ int batch_device_grouped(int64_t n, const int8_t *q, const int64_t *qoff, const 
                          const int32_t *gqlen_host);
 }  // namespace sw
 
+namespace stats {
+// The --blasttab columns of n reported search hits (stats_kernel.cu): hit d
+// of query query_of[d] (text at qtext + qoff_q[query]) against protein
+// protein[d] of the index text T (from pstart[protein]), residues mapped by
+// xmap; hits whose sw_status is not TPZ_SW_OK get -1 columns.  Waits for
+// its work on `st`.
+int reported_stats(int64_t n, const int8_t *qtext, const int64_t *qoff_q, const int32_t *query_of,
+                   const int8_t *T, const int64_t *pstart, const int32_t *protein,
+                   const int32_t *raw, const int32_t *qend, const int32_t *send,
+                   const int32_t *sw_status, const int8_t *mat, const int8_t *xmap, int go, int ge,
+                   int32_t *qstart, int32_t *sstart, int32_t *length, int32_t *gapopen,
+                   int32_t *mismatch, double *identity, cudaStream_t st);
+}  // namespace stats
+
 }  // namespace tpz

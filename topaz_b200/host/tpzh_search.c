@@ -23,6 +23,7 @@
 #include "../../include/topaz_b200.h"
 
 #include <errno.h>
+#include <time.h>
 #include <fcntl.h>
 #include <inttypes.h>
 #include <math.h>
@@ -133,7 +134,17 @@ typedef struct {
     int64_t next_read, next_print;
     int done;
     uint64_t nonzero, total_hits;
+    /* time spent, summed over batches (under mu): device stages of
+     * tpz_search_batch (seed + chains, walk + hitlist, SW + ranking), the
+     * batch calls' wall time, host ingest (SEG + alphabet) and formatting */
+    double dev_ms[3], call_s, ingest_s, format_s;
 } search_ctx;
+
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + ts.tv_nsec * 1e-9;
+}
 
 /* A --blasttab line: query, hit, ranking values and its statistics. */
 typedef struct {
@@ -193,13 +204,21 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
     char *cat = malloc(total + 1);
     for (int64_t i = 0; i < nq; ++i) memcpy(cat + qoff[i], qs[i].seq, qs[i].len);
     /* run_seg + seq_2internal for the whole batch over host threads */
+    const double t_in = now_s();
     tpz_prepare_queries(cat, qoff, qlen, nq, o->seg_enabled, c->prep_threads);
     for (int64_t i = 0; i < nq; ++i) memcpy(qs[i].seq, cat + qoff[i], qs[i].len);
     tpz_search_result *res = NULL;
+    const double t_call = now_s();
     if (tpz_search_batch(c->ix, cat, qoff, qlen, nq, c->so, &res) != 0) {
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         exit(EXIT_FAILURE);
     }
+    const double t_fmt = now_s();
+    pthread_mutex_lock(&c->mu);
+    for (int k = 0; k < 3; ++k) c->dev_ms[k] += res->stage_ms[k];
+    c->ingest_s += t_call - t_in;
+    c->call_s += t_fmt - t_call;
+    pthread_mutex_unlock(&c->mu);
     int64_t maxh = 1;
     for (int64_t q = 0; q < nq; ++q) {
         const int64_t nh = res->hit_off[q + 1] - res->hit_off[q];
@@ -258,7 +277,19 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
         }
         if (count) { (*nonzero)++; *total_hits += count; }
     }
-    if (nlines) {
+    if (nlines && res->qstart) {
+        /* the statistics came with the batch (computed on the device) */
+        for (int64_t i = 0; i < nlines; ++i) {
+            line_t *ln = &lines[i];
+            const int64_t h = ln->h;
+            ln->st.qstart = res->qstart[h];
+            ln->st.sstart = res->sstart[h];
+            ln->st.length = res->length[h];
+            ln->st.mismatch = res->mismatch[h];
+            ln->st.gapopen = res->gapopen[h];
+            ln->st.identity = res->sw_status[h] == TPZ_SW_OK ? res->identity[h] : INFINITY;
+        }
+    } else if (nlines) {
         /* statistics over host threads, then the lines in order */
         int nt = c->prep_threads < 1 ? 1 : c->prep_threads;
         if (nt > nlines) nt = (int)nlines;
@@ -279,6 +310,8 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
         stats_worker(&jobs[0]);
         for (int t = 1; t < nt; ++t)
             if (running[t]) pthread_join(th[t], NULL);
+    }
+    if (nlines) {
         for (int64_t i = 0; i < nlines; ++i) {
             const line_t *ln = &lines[i];
             const int64_t q = ln->q, h = ln->h;
@@ -296,6 +329,9 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
     free(rk); free(tmp);
     tpz_search_result_free(res);
     free(cat); free(qoff); free(qlen);
+    pthread_mutex_lock(&c->mu);
+    c->format_s += now_s() - t_fmt;
+    pthread_mutex_unlock(&c->mu);
 }
 
 /* Worker: take the next batch from the FASTA reader (batch ids in reading
@@ -388,11 +424,14 @@ load_fail:
         return -1;
     }
     tpz_index *ix = NULL;
+    const double t_up = now_s();
     if (tpz_index_create((const uint8_t *)T.data, (int64_t)T.size, (const int64_t *)SA.data, ind.data,
                          (int64_t)Psize, &ix) != 0) {
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         return -1;
     }
+    const double upload_s = now_s() - t_up;
+    const double t_search = now_s();
     const rec_t *recs = (const rec_t *)ind.data;
     init_int2idx();
 
@@ -414,6 +453,8 @@ load_fail:
      * Karlin parameters are outside what it takes (k <= 0, NaN -E) */
     const int report = o->k > 0 && o->evalue == o->evalue;
     if (report) {
+        /* --blasttab columns of the printed hits on the device */
+        so.blasttab_stats = o->superfast ? 0 : 1;
         so.report_hits = o->num_hits;
         so.max_evalue = o->evalue;
         so.lambda = o->lambda;
@@ -450,6 +491,11 @@ load_fail:
     tpz_index_destroy(ix);
     gettimeofday(&t1, NULL);
     fprintf(stderr, "output %" PRIu64 " hits for %" PRIu64 " queries\n", total_hits, nonzero);
+    fprintf(stderr, "timing: index upload %.2f s, queries %.2f s (%d host threads; summed over "
+            "batches: ingest %.2f s, batch calls %.2f s, format %.2f s; device seed %.0f ms, walk "
+            "%.0f ms, SW + ranking %.0f ms)\n",
+            upload_s, now_s() - t_search, nw, c.ingest_s, c.call_s, c.format_s, c.dev_ms[0],
+            c.dev_ms[1], c.dev_ms[2]);
     fprintf(stderr, "elapsed time: %.1f seconds\n",
             ((t1.tv_sec - t0.tv_sec) * 1000.0 + (t1.tv_usec - t0.tv_usec) / 1000.0) / 1000);
     fprintf(stderr, "done!\n");

@@ -148,7 +148,8 @@ class _SearchOpts(ctypes.Structure):
                 ("mat625", _VP), ("trace_pops", ctypes.c_int64),
                 ("report_hits", ctypes.c_int32), ("max_evalue", ctypes.c_double),
                 ("lam", ctypes.c_double), ("k", ctypes.c_double), ("H", ctypes.c_double),
-                ("db_size", ctypes.c_uint64), ("db_proteins", ctypes.c_uint64)]
+                ("db_size", ctypes.c_uint64), ("db_proteins", ctypes.c_uint64),
+                ("blasttab_stats", ctypes.c_int32)]
 
 
 _P64 = ctypes.POINTER(ctypes.c_int64)
@@ -167,7 +168,9 @@ class _SearchResult(ctypes.Structure):
                 ("evalue", ctypes.POINTER(ctypes.c_double)),
                 ("sw_pairs", ctypes.c_int64), ("sw_cells", ctypes.c_int64),
                 ("seed_ms", ctypes.c_double), ("chain_ms", ctypes.c_double),
-                ("positions", ctypes.c_int64)]
+                ("positions", ctypes.c_int64), ("qstart", _P32), ("sstart", _P32),
+                ("length", _P32), ("gapopen", _P32), ("mismatch", _P32),
+                ("identity", ctypes.POINTER(ctypes.c_double))]
 
 
 def _search_sigs(L):
@@ -257,8 +260,10 @@ class Index:
         qend, send, sw_status; optional trace_*).
 
         report: None for every hit in traversal order, or a dict with
-        max_evalue (and optionally hits, lam, k, H, db_size, db_proteins) for
-        the ranked, E-value-cut top hits with bitscore and evalue arrays."""
+        max_evalue (and optionally hits, lam, k, H, db_size, db_proteins,
+        stats) for the ranked, E-value-cut top hits with bitscore and evalue
+        arrays; with stats=True also the --blasttab columns (qstart, sstart,
+        length, gapopen, mismatch, identity) computed on the device."""
         L = lib()
         cat, off, lens = _concat(queries)
         mat = np.ascontiguousarray(mat, dtype=np.int8)
@@ -273,6 +278,7 @@ class Index:
             o.H = float(report.get("H", 0.140))
             o.db_size = int(report.get("db_size", T - P))
             o.db_proteins = int(report.get("db_proteins", P))
+            o.blasttab_stats = 1 if report.get("stats") else 0
         res = ctypes.POINTER(_SearchResult)()
         check(L.tpz_search_batch(self.handle, _p(cat), _p(off), _p(lens), len(queries),
                                  ctypes.byref(o), ctypes.byref(res)))
@@ -295,6 +301,9 @@ class Index:
             if report is not None:
                 out["bitscore"] = arr(r.bitscore, nh)
                 out["evalue"] = arr(r.evalue, nh)
+                if report.get("stats"):
+                    for k in ("qstart", "sstart", "length", "gapopen", "mismatch", "identity"):
+                        out[k] = arr(getattr(r, k), nh)
             if trace_pops:
                 out["trace_n"] = arr(r.trace_n, nq)
                 for k in ("trace_row", "trace_off", "trace_score", "trace_len", "trace_counted"):
