@@ -56,6 +56,8 @@ def test_sa_search_shim_every_output_matches_reference(both):
     for q in qs:
         for off in range(0, len(q) - 5, 3):
             for length in (0, 1, 3, 6, 12):
+                if off + length > len(q):
+                    continue                   # sa_search would read past the query
                 w, g = _search(R, h, L, ix, q, off, length)
                 assert w == g, (off, length)
                 n += 1
