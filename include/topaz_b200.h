@@ -245,6 +245,11 @@ typedef struct {
     /* report mode only: 1 = also the --blasttab columns of every reported
      * hit on the device (ssw_align_stats, src/ssw.c:900-978) */
     int32_t blasttab_stats;
+    /* 0: queries come in the internal alphabet (after run_seg +
+     * seq_2internal); 1: they come as upper-case residues and are SEG-masked
+     * and mapped on the device (tpz_prepare_queries_device); 2: the same
+     * without SEG (-M) */
+    int32_t ingest;
 } tpz_search_opts;
 
 typedef struct {
@@ -284,6 +289,15 @@ TPZ_API void tpz_search_result_free(tpz_search_result *r);
  * nthreads host threads. */
 TPZ_API int tpz_prepare_queries(char *cat, const int64_t *off, const int32_t *len, int64_t n,
                                 int seg, int nthreads);
+
+/* The same ingest on the device, in place: query i = cat[off[i] ..
+ * off[i]+len[i]) in device memory (upper-case residues in, internal
+ * alphabet out; queries disjoint, total_bytes = the extent of cat they
+ * use).  SEG's doubles are computed from the host's tables with separately
+ * rounded operations, so the masks equal tpz_prepare_queries' bit for bit.
+ * Work goes on `stream`; the call waits for it. */
+TPZ_API int tpz_prepare_queries_device(char *cat, const int64_t *off, const int32_t *len,
+                                       int64_t n, int64_t total_bytes, int seg, void *stream);
 
 /* Suffix array of the .psq bytes T[0, n) on the device, for `topaz index`
  * (divsufsort64 in serif_index, src/index.c:24-93, builds it on the host):

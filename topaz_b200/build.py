@@ -19,7 +19,10 @@ LIB = os.path.join(LIBDIR, "libtopaz_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["tpz_common.cu", "sw_kernel.cu", "search_kernels.cu", "search_host.cu", "sa_build.cu", "ssw_shim.cu",
-           "stats_kernel.cu"]
+           "stats_kernel.cu", "seg_kernel.cu"]
+# per-file nvcc flags: the device SEG must round every double operation
+# separately (no fused multiply-adds), as the host code does
+EXTRA_FLAGS = {"seg_kernel.cu": ["-fmad=false"]}
 HOSTDIR = os.path.join(HERE, "host")
 HOST_SOURCES = ["tpzh_fasta.c", "tpzh_seg.c", "tpzh_index.c", "tpzh_stats.c",
                 "tpzh_search.c", "tpzh_main.c", "tpzh_prepare.c"]
@@ -57,7 +60,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
                "--default-stream", "per-thread",
-               "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+               "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj,
+               *EXTRA_FLAGS.get(os.path.basename(src), [])]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))

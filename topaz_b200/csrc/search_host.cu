@@ -845,8 +845,36 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     std::vector<int32_t> qstatus(nq, 0), qlen_eff(nq);
     int64_t bytes = 0;
     int max_cap = 1, max_cursors = 1;
+    if (o->ingest < 0 || o->ingest > 2) {
+        tpz::set_error("tpz_search_batch: ingest must be 0, 1 or 2");
+        return TPZ_E_ARG;
+    }
+    // raw residues (ingest 1/2) go to the device packed, one query after
+    // the other, and are masked and mapped there
+    std::vector<char> packed;
+    std::vector<int64_t> packed_off;
+    if (o->ingest) {
+        int64_t tot = 0;
+        for (int64_t q = 0; q < nq; ++q) {
+            if (qlen[q] < 0 || qoff[q] < 0) {
+                tpz::set_error("tpz_search_batch: negative query offset or length");
+                return TPZ_E_ARG;
+            }
+            tot += qlen[q];
+        }
+        packed.resize(tot + 1);
+        packed_off.resize(nq);
+        tot = 0;
+        for (int64_t q = 0; q < nq; ++q) {
+            memcpy(packed.data() + tot, qcat + qoff[q], qlen[q]);
+            packed_off[q] = tot;
+            tot += qlen[q];
+        }
+        qcat = packed.data();
+        qoff = packed_off.data();
+    }
     for (int64_t q = 0; q < nq; ++q) {
-        if (qlen[q] < 0 || qoff[q] < 0 || !letters_ok(qcat + qoff[q], qlen[q])) {
+        if (qlen[q] < 0 || qoff[q] < 0 || (!o->ingest && !letters_ok(qcat + qoff[q], qlen[q]))) {
             tpz::set_error("tpz_search_batch: queries must be internal letters 'A'..'Y'");
             return TPZ_E_ARG;
         }
@@ -893,6 +921,12 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     TPZ_CUDA(cudaMemcpy(dcb, cur_base.data(), 8 * (nq + 1), cudaMemcpyHostToDevice));
     TPZ_CUDA(cudaMemcpy(dqs, qstatus.data(), 4 * nq, cudaMemcpyHostToDevice));
     TPZ_CUDA(cudaMemcpy(dsub, sub, 625, cudaMemcpyHostToDevice));
+    if (o->ingest) {
+        // SEG (ingest 1) and the internal alphabet on the device; queries
+        // past the length limit have length 0 here and stay as they are
+        rc = tpz_prepare_queries_device((char *)dq, dqo, dql, nq, bytes, o->ingest == 1, nullptr);
+        if (rc) return rc;
+    }
 
     const int nsm = tpz::sm_count();
     struct timeval tw0, tw1;

@@ -50,6 +50,9 @@ TPZH_API int tpzh_header_id(const char *buf, int len, const char **id);
 /* hard-masks low-complexity regions of upper-cased residues with 'X'
  * (run_seg, src/seg_wrapper.c:15-49); returns the number of segments */
 TPZH_API int tpzh_seg_mask(char *seq, int len);
+/* the tables the device SEG computes with (ent_full 13, logxr 13 x 13,
+ * lnfac n entries), from the same functions as tpzh_seg_mask */
+TPZH_API void tpzh_seg_tables(double *ent_full, double *logxr, double *lnfac_out, int n);
 
 /* ---------------------------------------------------------------- index */
 /* `topaz index -f FASTA -p PREFIX` (serif_index, src/index.c:24-93) */

@@ -203,13 +203,20 @@ static void search_batch(search_ctx *c, query_t *qs, int64_t nq, FILE *out, uint
     for (int64_t i = 0; i < nq; ++i) { qoff[i] = total; qlen[i] = qs[i].len; total += qs[i].len; }
     char *cat = malloc(total + 1);
     for (int64_t i = 0; i < nq; ++i) memcpy(cat + qoff[i], qs[i].seq, qs[i].len);
-    /* run_seg + seq_2internal for the whole batch over host threads */
+    /* run_seg + seq_2internal: on the device inside the batch call when the
+     * statistics are computed there too (report mode), else over host
+     * threads (the host statistics read the prepared queries) */
     const double t_in = now_s();
-    tpz_prepare_queries(cat, qoff, qlen, nq, o->seg_enabled, c->prep_threads);
-    for (int64_t i = 0; i < nq; ++i) memcpy(qs[i].seq, cat + qoff[i], qs[i].len);
+    tpz_search_opts so = *c->so;
+    if (c->report) {
+        so.ingest = o->seg_enabled ? 1 : 2;
+    } else {
+        tpz_prepare_queries(cat, qoff, qlen, nq, o->seg_enabled, c->prep_threads);
+        for (int64_t i = 0; i < nq; ++i) memcpy(qs[i].seq, cat + qoff[i], qs[i].len);
+    }
     tpz_search_result *res = NULL;
     const double t_call = now_s();
-    if (tpz_search_batch(c->ix, cat, qoff, qlen, nq, c->so, &res) != 0) {
+    if (tpz_search_batch(c->ix, cat, qoff, qlen, nq, &so, &res) != 0) {
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         exit(EXIT_FAILURE);
     }

@@ -258,3 +258,24 @@ int tpzh_seg_mask(char *seq, int len) {
     free(l.v);
     return n;
 }
+
+/* The tables the device SEG uses (so that its doubles equal these):
+ * ent_full[0..12] the full-window entropy terms, logxr[t * 13 + x] =
+ * log(x * (1 / t)) for 1 <= x <= t <= 12 (the partial-window terms of
+ * sv_entropy), lnfac[0..n) ln n! as rounded here. */
+void tpzh_seg_tables(double *ent_full, double *logxr, double *lnfac_out, int n) {
+    seg_init();
+    for (int i = 0; i <= SEG_WINDOW; ++i) ent_full[i] = i ? entropy_full[i] : 0.0;
+    for (int t = 0; t <= SEG_WINDOW; ++t)
+        for (int x = 0; x <= SEG_WINDOW; ++x) {
+            double v = 0.0;
+            if (t >= 1 && x >= 1 && x <= t) {
+                const double rt = 1. / (double)t;
+                const double xd = x;
+                v = log(xd * rt);
+            }
+            logxr[t * (SEG_WINDOW + 1) + x] = v;
+        }
+    for (int i = 0; i < n; ++i) lnfac_out[i] = lnfac(i);
+}
+

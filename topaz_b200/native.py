@@ -149,7 +149,7 @@ class _SearchOpts(ctypes.Structure):
                 ("report_hits", ctypes.c_int32), ("max_evalue", ctypes.c_double),
                 ("lam", ctypes.c_double), ("k", ctypes.c_double), ("H", ctypes.c_double),
                 ("db_size", ctypes.c_uint64), ("db_proteins", ctypes.c_uint64),
-                ("blasttab_stats", ctypes.c_int32)]
+                ("blasttab_stats", ctypes.c_int32), ("ingest", ctypes.c_int32)]
 
 
 _P64 = ctypes.POINTER(ctypes.c_int64)
@@ -253,7 +253,7 @@ class Index:
         return sc, ln
 
     def search(self, queries, mat, num_hits=100, gap_open=11, gap_extend=1, min_hit_length=5,
-               seeds=300000, alignments=5000, trace_pops=0, report=None):
+               seeds=300000, alignments=5000, trace_pops=0, report=None, ingest=0):
         """Runs a batch of queries (internal-alphabet bytes).  Returns a dict
         of numpy arrays (per query: hit_off, npops, ncounted, status; per hit:
         protein, gapless_score, gapless_length, suffix_offset, rawscore,
@@ -269,6 +269,7 @@ class Index:
         mat = np.ascontiguousarray(mat, dtype=np.int8)
         o = _SearchOpts(num_hits, gap_open, gap_extend, min_hit_length, seeds, alignments,
                         _p(mat), trace_pops)
+        o.ingest = int(ingest)
         if report is not None:
             T, P = len(self._T), len(self._ind)
             o.report_hits = int(report.get("hits", num_hits))
