@@ -281,6 +281,12 @@ TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_
                              tpz_search_result **out);
 TPZ_API void tpz_search_result_free(tpz_search_result *r);
 
+/* Upper estimate of the device memory one query of length qlen takes inside
+ * tpz_search_batch with options o (no reference counterpart): for callers
+ * that admit queries against a memory budget (a serving loop).  -1 on bad
+ * arguments. */
+TPZ_API int64_t tpz_search_query_device_bytes(int32_t qlen, const tpz_search_opts *o);
+
 /* Query ingest of a batch, in place (run_seg + seq_2internal,
  * src/engine.c:250-277): query i = cat[off[i] .. off[i]+len[i]) holds
  * upper-case residues (as the FASTA reader gives them); with seg != 0 SEG

@@ -811,6 +811,28 @@ int tpz_sa_hsp(const tpz_index *db, const char *q, int32_t qlen, int32_t qoffset
                             gapless_score, gapless_length);
 }
 
+int64_t tpz_search_query_device_bytes(int32_t qlen, const tpz_search_opts *o) {
+    using namespace tpz::search;
+    if (!o || qlen < 0) return -1;
+    // the per-query share of tpz_search_batch's device buffers, with the
+    // capacities it sizes them by: cursors with their chain caches, protein
+    // caches and queue links per searched position; the hitlist scratch
+    // (score-bucket lists, hit slots, the protein hash); the hit records;
+    // and, per hit, the Smith-Waterman pair and result arrays
+    const int64_t ql = qlen > TPZ_SEARCH_MAX_QLEN ? 0 : qlen;
+    const int cap = qlen > 3000 ? (int)(1.5 * o->num_hits) : o->alignments;
+    const int64_t npos = std::max<int64_t>(0, ql - o->min_hit_length);
+    int hash_size = 16;
+    while (hash_size < 2 * (cap + 1)) hash_size <<= 1;
+    auto al = [](size_t x) { return (int64_t)((x + 15) & ~(size_t)15); };
+    const size_t ns = (size_t)cap + 1;
+    const int64_t per_q = 7 * al(4 * ns) + 2 * al(4 * (size_t)kSMax) + al(8 * (kSMax / 64)) +
+                          2 * al(4 * (size_t)hash_size);
+    const int64_t per_pos = 2 * ((int64_t)sizeof(Cursor) + 4 + 2 * 4 * kChain);
+    const int64_t per_hit = (int64_t)sizeof(Hit) + 2 * 8 + 18 * 4;
+    return (int64_t)qlen + per_q + npos * per_pos + (int64_t)cap * per_hit + 256;
+}
+
 int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
                      const int32_t *qlen, int64_t nq, const tpz_search_opts *o,
                      tpz_search_result **out) {

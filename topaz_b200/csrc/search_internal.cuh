@@ -106,11 +106,12 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
                    int score_only, const int32_t *subset = nullptr, int64_t nsub = 0,
-                   int known_multi_maxn = -1);
+                   int known_multi_maxn = -1, int lane = 0);
 // known_multi_maxn >= 0: the caller knows the longest subject among pairs
 // with queries longer than one 1,024-row stripe (0: no such pair), so the
 // call need not read it back from the device before sizing the stripe
-// boundary buffer (no host wait inside the call).
+// boundary buffer (no host wait inside the call).  lane 0/1: calls of one
+// host thread that run concurrently use different lanes (own streams).
 // The same for pairs grouped by query (group g = pairs [gstart[g],
 // gstart[g+1]), all with query length gqlen[g]): groups with enough pairs go
 // to the query-major kernels, one shared profile per query; the rest by pair.

@@ -764,11 +764,14 @@ struct LaunchCfgs {
     }
 };
 
-static int launch_cfg(const LaunchCfg **out) {
+// lane: calls of one thread that run at the same time (the chunks of the
+// host entry point) take different lanes, so they get separate streams
+static int launch_cfg(const LaunchCfg **out, int lane = 0) {
     static thread_local LaunchCfgs cfgs;
     std::vector<LaunchCfg *> &per_dev = cfgs.per_dev;
     int dev = 0;
     TPZ_CUDA(cudaGetDevice(&dev));
+    dev = 2 * dev + (lane & 1);
     if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, nullptr);
     if (!per_dev[dev]) {
         LaunchCfg *c = new LaunchCfg();
@@ -912,7 +915,8 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
                    const int8_t *s, const int64_t *soff, const int32_t *slen, const int8_t *mat,
                    int go, int ge, int32_t *score, int32_t *ref_end, int32_t *read_end,
                    int32_t *status, cudaStream_t st, const int8_t *xq, const int8_t *xs,
-                   int score_only, const int32_t *subset, int64_t nsub, int known_multi_maxn) {
+                   int score_only, const int32_t *subset, int64_t nsub, int known_multi_maxn,
+                   int lane) {
     g_last_launches = 0;
     if (subset && nsub == 0) return TPZ_OK;
     if (n < 0 || n > INT32_MAX / 3 || !mat) { set_error("tpz_sw_batch: bad n or matrix"); return TPZ_E_ARG; }
@@ -926,7 +930,7 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
         return TPZ_E_ARG;
     }
     const LaunchCfg *cfg = nullptr;
-    int rc = launch_cfg(&cfg);
+    int rc = launch_cfg(&cfg, lane);
     if (rc) return rc;
 
     // workspace: counts, cursor, rinfo, next_task, rerun_count, multi_maxn,
@@ -1222,13 +1226,14 @@ int batch_device(int64_t n, const int8_t *q, const int64_t *qoff, const int32_t 
 namespace {
 
 // Grow-only device buffers reused by the host entry point, and its streams:
-// one for the kernels, one for host-to-device and one for device-to-host
-// copies, so that a chunk's copies run beside another chunk's kernels.
+// two for the kernels (one per chunk), one for host-to-device and one for
+// device-to-host copies, so that a chunk's copies run beside another
+// chunk's kernels.
 struct HostBatchBuffers {
     void *p = nullptr;
     size_t cap = 0;
     int dev = -1;
-    cudaStream_t compute = nullptr, h2d = nullptr, d2h = nullptr;
+    cudaStream_t compute = nullptr, compute2 = nullptr, h2d = nullptr, d2h = nullptr;
     cudaEvent_t ev[8] = {};
 };
 thread_local HostBatchBuffers g_hb;
@@ -1239,13 +1244,15 @@ int ensure(size_t bytes) {
     if (g_hb.compute && g_hb.dev != dev) {
         // streams and events belong to the device they were made on
         cudaStreamDestroy(g_hb.compute);
+        cudaStreamDestroy(g_hb.compute2);
         cudaStreamDestroy(g_hb.h2d);
         cudaStreamDestroy(g_hb.d2h);
         for (cudaEvent_t &e : g_hb.ev) { cudaEventDestroy(e); e = nullptr; }
-        g_hb.compute = g_hb.h2d = g_hb.d2h = nullptr;
+        g_hb.compute = g_hb.compute2 = g_hb.h2d = g_hb.d2h = nullptr;
     }
     if (!g_hb.compute) {
         TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.compute, cudaStreamNonBlocking));
+        TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.compute2, cudaStreamNonBlocking));
         TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.h2d, cudaStreamNonBlocking));
         TPZ_CUDA(cudaStreamCreateWithFlags(&g_hb.d2h, cudaStreamNonBlocking));
         for (cudaEvent_t &e : g_hb.ev) TPZ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1358,19 +1365,20 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         return TPZ_E_ARG;
     }
     if (n == 0) return TPZ_OK;
-    // Pairs go in up to three chunks of growing size (1/32, then up to 1/5,
-    // then the rest): the kernels of a chunk run while the residues of the
-    // next ones are copied in, and a chunk's results are copied out while
-    // later chunks compute, so only the first, small copy is not hidden.
-    int64_t cut[4] = {0, n, n, n};
+    // Pairs go in two chunks when there are many: the first eighth, then the
+    // rest.  The first chunk's kernels run while the rest is copied in, and
+    // the two chunks run on separate streams (lanes), so the second chunk's
+    // kernels fill the GPU while the first chunk's last tasks finish; each
+    // chunk's results are copied out as soon as they are done.
+    int64_t cut[3] = {0, n, n};
     int nch = 1;
     if (n >= 65536) {
-        cut[1] = n / 32; cut[2] = n / 5; cut[3] = n;
-        nch = 3;
+        cut[1] = n / 8; cut[2] = n;
+        nch = 2;
     }
     // host-side validation and the byte ranges each chunk reads, chunks
     // scanned on their own threads
-    Span sp[3];
+    Span sp[2];
     {
         std::vector<std::thread> th;
         for (int c = 1; c < nch; ++c)
@@ -1407,7 +1415,7 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
     int32_t *dre = (int32_t *)d; d += b4;
     int32_t *drd = (int32_t *)d; d += b4;
     int32_t *dst = (int32_t *)d; d += b4;
-    cudaStream_t cs = g_hb.compute, hs = g_hb.h2d, os = g_hb.d2h;
+    cudaStream_t cst[2] = {g_hb.compute, g_hb.compute2}, hs = g_hb.h2d, os = g_hb.d2h;
     // The device copies of q and s keep the host offsets.  Each chunk copies
     // the part of its byte range not copied yet: the copied part is kept as
     // one interval [lo, hi) that grows to cover every range seen (a gap
@@ -1431,7 +1439,7 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         }
         return e;
     };
-    cudaEvent_t *in_ready = g_hb.ev, *done = g_hb.ev + 3;
+    cudaEvent_t *in_ready = g_hb.ev, *done = g_hb.ev + 2;
     for (int c = 0; c < nch; ++c) {
         const int64_t a = cut[c], m = cut[c + 1] - cut[c];
         TPZ_CUDA(copy_new(q, dq, sp[c].qlo, sp[c].qhi, qc_lo, qc_hi));
@@ -1444,14 +1452,16 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
     }
     for (int c = 0; c < nch; ++c) {
         const int64_t a = cut[c], m = cut[c + 1] - cut[c];
+        cudaStream_t cs = cst[c];
         TPZ_CUDA(cudaStreamWaitEvent(cs, in_ready[c], 0));
         rc = tpz::sw::batch_device_x(m, dq, dqoff + a, dqlen + a, ds, dsoff + a, dslen + a,
                                      mat625, gap_open, gap_extend, dsc + a, dre + a, drd + a,
                                      dst + a, cs, nullptr, nullptr, 0, nullptr, 0,
-                                     sp[c].multi_maxn);
+                                     sp[c].multi_maxn, c);
         if (rc) {
             cudaStreamSynchronize(hs);
-            cudaStreamSynchronize(cs);
+            cudaStreamSynchronize(cst[0]);
+            cudaStreamSynchronize(cst[1]);
             return rc;
         }
         TPZ_CUDA(cudaEventRecord(done[c], cs));
@@ -1462,7 +1472,8 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         TPZ_CUDA(cudaMemcpyAsync(status + a, dst + a, 4 * m, cudaMemcpyDeviceToHost, os));
     }
     TPZ_CUDA(cudaStreamSynchronize(os));
-    TPZ_CUDA(cudaStreamSynchronize(cs));
+    TPZ_CUDA(cudaStreamSynchronize(cst[0]));
+    TPZ_CUDA(cudaStreamSynchronize(cst[1]));
     return TPZ_OK;
 }
 

@@ -188,6 +188,8 @@ def _search_sigs(L):
     L.tpz_karlin.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double,
                              ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.tpz_search_query_device_bytes.argtypes = [ctypes.c_int32, ctypes.POINTER(_SearchOpts)]
+    L.tpz_search_query_device_bytes.restype = ctypes.c_int64
     L._search_sigs = True
 
 
@@ -312,6 +314,18 @@ class Index:
             return out
         finally:
             L.tpz_search_result_free(res)
+
+
+def query_device_bytes(qlen, num_hits=100, alignments=5000, min_hit_length=5,
+                       seeds=300000, gap_open=11, gap_extend=1):
+    """tpz_search_query_device_bytes: device memory of one query in a batch."""
+    L = lib()
+    _search_sigs(L)
+    o = _SearchOpts(num_hits, gap_open, gap_extend, min_hit_length, seeds, alignments, None, 0)
+    v = L.tpz_search_query_device_bytes(int(qlen), ctypes.byref(o))
+    if v < 0:
+        raise TopazError(-1, "bad arguments")
+    return int(v)
 
 
 def karlin(qlen, db_size, db_proteins, raw, lam=0.267, k=0.041, H=0.14):

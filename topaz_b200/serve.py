@@ -30,18 +30,11 @@ from . import native
 def query_device_bytes(qlen: int, num_hits: int = 100, alignments: int = 5000,
                        min_hit_length: int = 5) -> int:
     """Upper estimate of the device memory one query takes inside
-    tpz_search_batch: cursors, chain caches and queue links per searched
-    position, the hitlist structures and the hit and SW arrays of its
-    hitlist capacity."""
-    cap = int(1.5 * num_hits) if qlen > 3000 else alignments
-    npos = max(0, qlen - min_hit_length)
-    hash_size = 16
-    while hash_size < 2 * (cap + 1):
-        hash_size <<= 1
-    per_pos = 2 * (32 + 4 + 8 * 64) + 8          # cursor, queue link, 64 chain elements + proteins
-    hitlist = 7 * 4 * (cap + 1) + 2 * 4 * 4352 + 8 * 68 + 2 * 4 * hash_size
-    hits = cap * (16 + 4 * 24)
-    return npos * per_pos + hitlist + hits + qlen + 256
+    tpz_search_batch, from the library itself
+    (tpz_search_query_device_bytes: the same capacities the batch sizes its
+    buffers by)."""
+    return native.query_device_bytes(qlen, num_hits=num_hits, alignments=alignments,
+                                     min_hit_length=min_hit_length)
 
 
 class _Request:
