@@ -178,13 +178,13 @@ SEARCH_WORKLOAD = ("full search, mid size: 1,000,000-protein synthetic DB (log-n
 
 
 SERVE_WORKLOAD = ("serving on the resident mid-size DB: Poisson request arrivals at 5 offered "
-                  "loads (fractions of the measured batch throughput), each request 1-1000 "
+                  "loads (fractions of the loop's saturated throughput on this mix), each request 1-1000 "
                   "queries (log-uniform count) of 30-3000 residues, continuous batching across "
-                  "requests by %d worker threads (batches up to %d queries, admitted by free "
-                  "device memory), -H 100 -E 1e-3")
+                  "requests by %d worker threads (batches up to %d queries, both picked by the "
+                  "autotuner; admitted by free device memory), -H 100 -E 1e-3")
 
 
-def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.8, 1.0),
+def serve_bench(ix, mat, res, lens, batch_qps, args, loads=(0.2, 0.4, 0.6, 0.8, 1.0),
                 seconds=6.0):
     """p50/p99 request latency and delivered queries/s of the serving loop
     (topaz_b200.serve.SearchServer) at five offered loads."""
@@ -194,9 +194,12 @@ def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.
     qoff = np.cumsum(qlens) - qlens
     pool = native.prepare_queries([qres[o:o + n].tobytes() for o, n in zip(qoff, qlens)])
     rng = np.random.Generator(np.random.PCG64(args.seed + 22))
-    workers, max_batch = 3, 2000
-    srv = serve.SearchServer(ix, mat, workers=workers, max_batch=max_batch,
-                             report={"max_evalue": 1e-3})
+    # the loop's shape from the project's autotuner on a sample of this mix,
+    # and its capacity: saturated throughput on the same mix
+    rep = {"max_evalue": 1e-3}
+    (workers, max_batch), tried = serve.autotune(ix, mat, pool[:4000], report=rep)
+    capacity_qps = serve.saturated_qps(ix, mat, pool, workers, max_batch, report=rep)
+    srv = serve.SearchServer(ix, mat, workers=workers, max_batch=max_batch, report=rep)
     srv.submit(pool[:50]).result()                        # warm-up
     rows = []
     mean_req = float(np.mean(np.exp(rng.uniform(0, np.log(1000), 100000))))
@@ -222,6 +225,9 @@ def serve_bench(ix, mat, res, lens, capacity_qps, args, loads=(0.2, 0.4, 0.6, 0.
                      "p99_ms": round(float(np.percentile(lat, 99)), 2)})
     srv.close()
     return {"workload": SERVE_WORKLOAD % (workers, max_batch), "capacity_qps": round(capacity_qps, 1),
+            "capacity": "saturated throughput of the serving loop on this request mix",
+            "batch_capacity_qps_config2_mix": round(batch_qps, 1),
+            "autotune": {"%dx%d" % k: round(v, 1) for k, v in tried.items()},
             "loads": rows, "api": "topaz_b200.serve.SearchServer over tpz_search_batch report mode"}
 
 

@@ -308,17 +308,23 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
         uint32_t cmx = 0u, thr = 0u;
         if (j >= 0 && j < N) {
             uint32_t F = inF, Fm = inFm, D = diag;
+            // first every row's diagonal term and its gap-open candidate (they
+            // depend only on the previous column), then the F / Fm chains,
+            // the only row-to-row dependences, with E and H hanging off them
+            uint32_t Xa[R], Xga[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const uint32_t sc = prmt(cwa[r >> 2], cwb[r >> 2], SEL[r & 3]);
-                const uint32_t X = __viaddmax_s16x2_relu(D, sc, E[r]);
-                const uint32_t Hn = __vimax_s16x2_relu(X, F);
-                const uint32_t Xg = __viaddmax_s16x2(X, NGO, NEGINF);
-                const uint32_t Gp = __viaddmax_s16x2(Fm, ngo[r], Xg);
+                Xa[r] = __viaddmax_s16x2_relu(r == 0 ? D : H[r - 1], sc, E[r]);
+                Xga[r] = __viaddmax_s16x2(Xa[r], NGO, NEGINF);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t Hn = __vimax_s16x2_relu(Xa[r], F);
+                const uint32_t Gp = __viaddmax_s16x2(Fm, ngo[r], Xga[r]);
                 E[r] = __viaddmax_s16x2(E[r], NGE, Gp);
-                F = __viaddmax_s16x2(F, NGE, Xg);
-                Fm = __viaddmax_s16x2(Fm, nge[r], Xg);
-                D = H[r];
+                F = __viaddmax_s16x2(F, NGE, Xga[r]);
+                Fm = __viaddmax_s16x2(Fm, nge[r], Xga[r]);
                 H[r] = Hn;
             }
             // column maximum of the lane's rows, floored at the search
@@ -1365,15 +1371,15 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         return TPZ_E_ARG;
     }
     if (n == 0) return TPZ_OK;
-    // Pairs go in two chunks when there are many: the first eighth, then the
-    // rest.  The first chunk's kernels run while the rest is copied in, and
+    // Pairs go in two chunks when there are many: the first sixteenth, then
+    // the rest.  The first chunk's kernels run while the rest is copied in, and
     // the two chunks run on separate streams (lanes), so the second chunk's
     // kernels fill the GPU while the first chunk's last tasks finish; each
     // chunk's results are copied out as soon as they are done.
     int64_t cut[3] = {0, n, n};
     int nch = 1;
     if (n >= 65536) {
-        cut[1] = n / 8; cut[2] = n;
+        cut[1] = n / 16; cut[2] = n;
         nch = 2;
     }
     // host-side validation and the byte ranges each chunk reads, chunks

@@ -168,3 +168,35 @@ def latency_of(future) -> float:
     """Seconds from submit to completion of a finished request."""
     req = future.request
     return req.t_done - req.t_submit
+
+
+def saturated_qps(index, mat, queries, workers: int, max_batch: int, report=None,
+                  request_size: int = 250) -> float:
+    """Queries per second the serving loop delivers with every request
+    already waiting (its capacity on this query mix)."""
+    srv = SearchServer(index, mat, workers=workers, max_batch=max_batch, report=report)
+    try:
+        srv.submit(queries[:min(len(queries), 50)]).result()          # warm-up
+        t0 = time.perf_counter()
+        futs = [srv.submit(queries[i:i + request_size])
+                for i in range(0, len(queries), request_size)]
+        for f in futs:
+            f.result()
+        return len(queries) / (time.perf_counter() - t0)
+    finally:
+        srv.close()
+
+
+def autotune(index, mat, queries, report=None,
+             candidates=((2, 1000), (2, 2000), (3, 1000), (3, 2000), (4, 1000), (4, 2000),
+                         (3, 3000))):
+    """Picks the worker count and batch cap of the serving loop for this
+    index and query mix: the candidate with the highest saturated
+    throughput on `queries` (a sample of the expected requests).  Returns
+    ((workers, max_batch), {candidate: queries/s})."""
+    seen = {}
+    for w, b in candidates:
+        seen[(w, b)] = saturated_qps(index, mat, queries, w, b, report=report)
+    best = max(seen, key=seen.get)
+    return best, seen
+
