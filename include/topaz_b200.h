@@ -55,6 +55,12 @@ enum {
 };
 
 TPZ_API const char *tpz_last_error(void);
+
+/* Creates the CUDA context of the current device and sets up the device
+ * memory pool (no reference counterpart).  Optional: every entry point does
+ * this on first use; a program can call it early on a thread of its own so
+ * the start-up cost overlaps reading its input (`topaz search` does). */
+TPZ_API int tpz_device_init(void);
 TPZ_API const char *tpz_version(void);
 
 /* Substitution matrix by name: BLOSUM45/50/62/80/90, PAM30/70/250

@@ -164,3 +164,25 @@ def test_device_bytes_grow_with_query_length_and_capacity():
     assert serve.query_device_bytes(500, alignments=1500) < serve.query_device_bytes(500, alignments=5000)
     # long queries (> 3000) hold 1.5 x H hits, not -A
     assert serve.query_device_bytes(3001, num_hits=100) < serve.query_device_bytes(3000, num_hits=100) * 1.2
+
+
+def test_cancel_drops_waiting_queries_and_spares_other_requests():
+    rng = np.random.default_rng(31)
+    ix = FakeIndex(delay=0.05)
+    srv = serve.SearchServer(ix, np.zeros((25, 25), np.int8), workers=1, max_batch=10,
+                             mem_budget=1 << 40)
+    try:
+        big = _queries(rng, 200)
+        small = _queries(rng, 5)
+        f_big = srv.submit(big)
+        f_small = srv.submit(small)
+        time.sleep(0.02)                   # the first batch of the big request is running
+        assert srv.cancel(f_big)
+        assert f_big.cancelled()
+        res = f_small.result(timeout=10)
+        _same(res, small)
+        seen = sum(len(b) for b in ix.batches)
+        assert seen < len(big)             # most of the big request never reached the index
+        assert not srv.cancel(f_small)     # already done
+    finally:
+        srv.close()

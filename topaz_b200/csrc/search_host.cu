@@ -811,6 +811,15 @@ int tpz_sa_hsp(const tpz_index *db, const char *q, int32_t qlen, int32_t qoffset
                             gapless_score, gapless_length);
 }
 
+int tpz_device_init(void) {
+    // the primary context and the device pool settings, so that a caller
+    // can pay for them on another thread while it reads its input
+    TPZ_CUDA(cudaFree(nullptr));
+    tpz::sm_count();
+    keep_pool_memory();
+    return TPZ_OK;
+}
+
 int64_t tpz_search_query_device_bytes(int32_t qlen, const tpz_search_opts *o) {
     using namespace tpz::search;
     if (!o || qlen < 0) return -1;

@@ -384,9 +384,24 @@ static void *search_worker(void *arg) {
     return NULL;
 }
 
+static void *device_init_thread(void *arg) {
+    *(int *)arg = tpz_device_init();
+    return NULL;
+}
+
+/* the start-up thread is joined before the process ends on any path */
+static pthread_t g_init_th;
+static int g_init_started, g_init_rc;
+static void join_init(void) {
+    if (g_init_started) pthread_join(g_init_th, NULL);
+    g_init_started = 0;
+}
+
 int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     struct timeval t0, t1;
     gettimeofday(&t0, NULL);
+    /* the CUDA context comes up while the database files are mapped */
+    g_init_started = pthread_create(&g_init_th, NULL, device_init_thread, &g_init_rc) == 0;
     /* db_load / _load_index (src/db.c:34-122) in the same order, with the
      * same messages; a file that cannot be mapped ends the process with
      * engine_init's message (src/engine.c:47-50) */
@@ -398,6 +413,7 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     if (SA.size != T.size * 8) {
         fprintf(stderr, "Error: SA (%s.SA, %" PRIu64 " bytes) should be 8 x T (%s.psq, %" PRIu64 " bytes)!\nExiting...\n",
                 prefix, SA.size, prefix, T.size);
+        join_init();
         exit(EXIT_FAILURE);
     }
     if (map_file(prefix, ".phr", &phr)) goto load_fail;
@@ -414,11 +430,13 @@ int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     }
     if (ind.size != Psize * 24) {
         fprintf(stderr, "Error: index is the wrong size (read %" PRIu64 ", expected %" PRIu64 ")", ind.size, Psize * 24);
+        join_init();
         exit(EXIT_FAILURE);
     }
     if (0) {
 load_fail:
         fprintf(stderr, "Error: could not load database, %s\n", strerror(errno));
+        join_init();
         exit(EXIT_FAILURE);
     }
     const uint64_t db_size = T.size - Psize, db_proteins = Psize;
@@ -427,6 +445,12 @@ load_fail:
 
     int8_t mat[625];
     if (tpz_matrix(o->matrix, mat) != 0) {
+        fprintf(stderr, "Error: %s\n", tpz_last_error());
+        join_init();
+        return -1;
+    }
+    join_init();
+    if (g_init_rc != 0 && tpz_device_init() != 0) {   /* again here, for this thread's message */
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         return -1;
     }

@@ -38,7 +38,7 @@ def query_device_bytes(qlen: int, num_hits: int = 100, alignments: int = 5000,
 
 
 class _Request:
-    __slots__ = ("queries", "results", "left", "future", "t_submit", "t_done")
+    __slots__ = ("queries", "results", "left", "future", "t_submit", "t_done", "cancelled")
 
     def __init__(self, queries):
         self.queries = queries
@@ -47,6 +47,7 @@ class _Request:
         self.future = Future()
         self.t_submit = time.perf_counter()
         self.t_done = None
+        self.cancelled = False
 
 
 class SearchServer:
@@ -91,6 +92,21 @@ class SearchServer:
                 self._pending.append((req, i))
             self._cv.notify_all()
         return req.future
+
+    def cancel(self, future) -> bool:
+        """Cancels a request: its queries still waiting are dropped, a batch
+        already holding some of them finishes without handing them back, and
+        the future ends cancelled.  False when the request had completed."""
+        req = future.request
+        with self._cv:
+            if req.future.done():
+                return False
+            req.cancelled = True
+            self._pending = collections.deque(x for x in self._pending if x[0] is not req)
+            req.t_done = time.perf_counter()
+            ok = req.future.cancel()
+            self._cv.notify_all()
+        return ok
 
     def close(self):
         with self._cv:
@@ -146,6 +162,8 @@ class SearchServer:
                 self._mem_used -= need
                 self.batches.append((len(batch), dt))
                 for k, (req, i) in enumerate(batch):
+                    if req.cancelled:
+                        continue
                     if err is not None:
                         if not req.future.done():
                             req.t_done = time.perf_counter()
