@@ -749,7 +749,8 @@ int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     DevBuf b;
     uint8_t *dq; int64_t *dqo, *drow; int32_t *dql, *dqf, *doff, *dsc, *dln; int8_t *dsub;
     int rc;
-    if ((rc = b.alloc(&dq, bytes)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
+    // + 64: hsp_at's vector loads read up to 15 bytes past a query's end
+    if ((rc = b.alloc(&dq, bytes + 64)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
         (rc = b.alloc(&dqf, n)) || (rc = b.alloc(&doff, n)) || (rc = b.alloc(&drow, n)) ||
         (rc = b.alloc(&dsc, n)) || (rc = b.alloc(&dln, n)) || (rc = b.alloc(&dsub, 625)))
         return rc;
@@ -936,7 +937,8 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     Cursor *dcur; Hit *dhits; QueryOut *dqout; PopRec *dtrace = nullptr;
     int32_t *dqnext, *dcprot; uint32_t *dcache;
     int rc;
-    if ((rc = b.alloc(&dq, bytes + 1)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
+    // + 64: hsp_at's vector loads read up to 15 bytes past a query's end
+    if ((rc = b.alloc(&dq, bytes + 64)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
         (rc = b.alloc(&dpb, nq + 1)) || (rc = b.alloc(&dcb, nq + 1)) || (rc = b.alloc(&dqs, nq)) ||
         (rc = b.alloc(&dsub, 625)) || (rc = b.alloc(&dcur, 2 * npos + 1)) ||
         (rc = b.alloc(&dscratch, per_q * nq)) || (rc = b.alloc(&dhits, (size_t)nq * max_cap)) ||

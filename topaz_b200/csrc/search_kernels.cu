@@ -89,68 +89,67 @@ __device__ __forceinline__ int64_t protein_of(const DevIndex &ix, int64_t pos) {
     return (int64_t)ix.nl[pos >> 6] + newlines_in_block_before(ix.T, pos);
 }
 
+// Copies bytes [p, p + n) (n <= 64, any alignment) into a thread's 16-byte
+// aligned buffer with aligned 16-byte loads issued together -- one memory
+// round trip for up to 64 bytes instead of one per 8.  Returns the offset of
+// p in the buffer.  The loads may cover up to 15 bytes before p and after
+// p + n: callers keep 16 readable bytes around every window (the text and
+// query buffers are 256-byte aligned and padded at the end).
+__device__ __forceinline__ int stage64(const uint8_t *p, int n, uint4 *buf) {
+    const uintptr_t a = (uintptr_t)p & ~(uintptr_t)15;
+    const int o = (int)((uintptr_t)p - a);
+    const int nv = (o + n + 15) >> 4;
+    const uint4 *src = reinterpret_cast<const uint4 *>(a);
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        if (k < nv) buf[k] = __ldg(src + k);
+    return o;
+}
+
 // sa_hsp (src/search.c:99-190) at text position idx for query offset off.
 // Returns the length (-1 when the first symbols differ; score untouched then).
+// The windows (up to 128 bytes each side) are read 64 bytes at a time with
+// vector loads; the running sums walk them in the reference's order and stop
+// at the first '\n' exactly as its byte loop does.
 __device__ int hsp_at(const DevIndex &ix, int64_t idx, const uint8_t *Q, int qlen, int off,
                       const int8_t *sub, int *score) {
     const uint8_t *t = ix.T + idx;
     const uint8_t *q = Q + off;
     if (t[0] != q[0]) return -1;
+    uint4 tb[5], qb[5];
+    const uint8_t *tc = reinterpret_cast<const uint8_t *>(tb);
+    const uint8_t *qc = reinterpret_cast<const uint8_t *>(qb);
     int64_t mr = ix.Tsize - idx;
     if (mr > qlen - off) mr = qlen - off;
     if (mr > 128) mr = 128;
-    // bytes in chunks of 8: the loads of a chunk go out together (only
-    // bytes inside the window are read), then the running sum walks them
-    // in order and stops at the first '\n' exactly as the byte loop does
-    constexpr int kC = 8;
     int run = 0, best_r = 0, arg_r = 0;
-    for (int i = 0; i < (int)mr; i += kC) {
-        uint8_t c[kC], d[kC];
-#pragma unroll
-        for (int k = 0; k < kC; ++k) {
-            const bool in = i + k < (int)mr;
-            c[k] = in ? t[i + k] : (uint8_t)'\n';
-            d[k] = in ? q[i + k] : (uint8_t)'A';
+    bool stop = false;
+    for (int i0 = 0; i0 < (int)mr && !stop; i0 += 64) {
+        const int n = min(64, (int)mr - i0);
+        const int ot = stage64(t + i0, n, tb), oq = stage64(q + i0, n, qb);
+        for (int k = 0; k < n; ++k) {
+            const uint8_t c = tc[ot + k];
+            if (c == '\n') { stop = true; break; }
+            run += sub[(c - 'A') * 25 + (qc[oq + k] - 'A')];
+            if (run >= best_r) { best_r = run; arg_r = i0 + k; }
         }
-        bool stop = false;
-#pragma unroll
-        for (int k = 0; k < kC; ++k) {
-            if (!stop) {
-                if (c[k] == '\n') {
-                    stop = true;
-                } else {
-                    run += sub[(c[k] - 'A') * 25 + (d[k] - 'A')];
-                    if (run >= best_r) { best_r = run; arg_r = i + k; }
-                }
-            }
-        }
-        if (stop) break;
     }
     int64_t ml = idx < off ? idx : off;
     if (ml > 128) ml = 128;
     int best_l = 0, arg_l = 0;
     run = 0;
-    for (int i = 1; i < (int)ml; i += kC) {
-        uint8_t c[kC], d[kC];
-#pragma unroll
-        for (int k = 0; k < kC; ++k) {
-            const bool in = i + k < (int)ml;
-            c[k] = in ? t[-(i + k)] : (uint8_t)'\n';
-            d[k] = in ? q[-(i + k)] : (uint8_t)'A';
+    stop = false;
+    // left: i = 1 .. ml-1 reads t[-i]; a round stages t[-(i0+n-1) .. -i0]
+    for (int i0 = 1; i0 < (int)ml && !stop; i0 += 64) {
+        const int n = min(64, (int)ml - i0);
+        const int ot = stage64(t - (i0 + n - 1), n, tb), oq = stage64(q - (i0 + n - 1), n, qb);
+        for (int k = 0; k < n; ++k) {
+            // byte t[-(i0 + k)] sits at index n - 1 - k of the staged range
+            const uint8_t c = tc[ot + n - 1 - k];
+            if (c == '\n') { stop = true; break; }
+            run += sub[(c - 'A') * 25 + (qc[oq + n - 1 - k] - 'A')];
+            if (run >= best_l) { best_l = run; arg_l = i0 + k; }
         }
-        bool stop = false;
-#pragma unroll
-        for (int k = 0; k < kC; ++k) {
-            if (!stop) {
-                if (c[k] == '\n') {
-                    stop = true;
-                } else {
-                    run += sub[(c[k] - 'A') * 25 + (d[k] - 'A')];
-                    if (run >= best_l) { best_l = run; arg_l = i + k; }
-                }
-            }
-        }
-        if (stop) break;
     }
     *score = best_l + best_r;
     return arg_l + arg_r;
