@@ -246,6 +246,24 @@ def seed_roofline(positions, ms, tsize):
             "peak_source": src}
 
 
+def extension_roofline(chain_elems, chain_ms, refill_elems, pops):
+    """Gapless extension (sa_hsp) of the cursor chains against HBM:
+    algorithmic bytes per call = the 8-byte SA entry + the text window's
+    32-byte sectors, up to 8 (128 residues each side); the chain kernel's
+    calls over its device time.  Also how many of the computed extensions
+    the walk used (one per pop)."""
+    peak, src = measured_hbm_gbs()
+    gb = chain_elems * (8 + 8 * 32) / 1e9
+    ach = gb / (chain_ms / 1e3) if chain_ms > 0 else None
+    return {"chain_calls": int(chain_elems), "walk_refill_calls": int(refill_elems),
+            "device_ms": round(chain_ms, 2), "algorithmic_gb": round(gb, 2),
+            "achieved_gbs": round(ach, 1) if ach else None, "peak_gbs": peak,
+            "frac": round(ach / peak, 3) if ach and peak else None, "peak_source": src,
+            "bytes_per_call": "8 B SA entry + up to 8 x 32 B text sectors",
+            "computed_over_used": round((chain_elems + refill_elems) / max(pops, 1), 2),
+            "l2_hit_rate": "profiles/search_kernels_small.md (ncu)"}
+
+
 def measured_hbm_gbs():
     """(peak GB/s, where it comes from)"""
     try:
@@ -366,7 +384,7 @@ def search_bench(args, dev):
     torch.cuda.synchronize()
     stage = np.zeros(4)
     nh = [0]
-    swc = [0, 0, 0.0, 0.0, 0]
+    swc = [0, 0, 0.0, 0.0, 0, 0, 0]
     pops = []
     starts = list(range(0, len(q_aa), bsz))
     lock = threading.Lock()
@@ -389,6 +407,8 @@ def search_bench(args, dev):
                 swc[2] += r["seed_ms"]
                 swc[3] += r["chain_ms"]
                 swc[4] += r["positions"]
+                swc[5] += r["chain_elems"]
+                swc[6] += r["refill_elems"]
                 pops.extend(r["npops"].tolist())
 
     t0 = time.perf_counter()
@@ -415,6 +435,7 @@ def search_bench(args, dev):
            "sw_pairs_per_query": round(swc[0] / len(q_aa), 1),
            "sw_gcells": round(swc[1] / 1e9, 2),
            "seed_lookup": seed_roofline(swc[4], swc[2], len(db.T)),
+           "extension": extension_roofline(swc[5], swc[3], swc[6], int(np.sum(pops))),
            "pops_per_query": {"mean": round(float(np.mean(pops)), 1),
                               "p50": int(np.percentile(pops, 50)), "p99": int(np.percentile(pops, 99)),
                               "max": int(np.max(pops))},

@@ -280,6 +280,9 @@ typedef struct {
      * -1 columns for hits without a Smith-Waterman alignment */
     const int32_t *qstart, *sstart, *length, *gapopen, *mismatch;
     const double *identity;
+    /* gapless extensions (sa_hsp) of the cursor chains: precomputed for
+     * every queued cursor, and refilled by the walk */
+    int64_t chain_elems, refill_elems;
 } tpz_search_result;
 
 TPZ_API int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,

@@ -401,6 +401,7 @@ struct ResultHolder {
     std::vector<int32_t> st_qstart, st_sstart, st_length, st_gapopen, st_mismatch;
     std::vector<double> st_identity;
     int64_t sw_pairs = 0, sw_cells = 0;
+    int64_t chain_elems = 0, refill_elems = 0;
 };
 
 // Ranking tables of report mode.  The bitscore of a raw score does not
@@ -947,6 +948,9 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         (rc = b.alloc(&dcprot, (size_t)kChain * (2 * npos + 1))))
         return rc;
     if (o->trace_pops > 0 && (rc = b.alloc(&dtrace, (size_t)nq * o->trace_pops))) return rc;
+    unsigned long long *dqueued;
+    if ((rc = b.alloc(&dqueued, 1))) return rc;
+    TPZ_CUDA(cudaMemset(dqueued, 0, sizeof(unsigned long long)));
     TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
     TPZ_CUDA(cudaMemcpy(dqo, qoff, 8 * nq, cudaMemcpyHostToDevice));
     TPZ_CUDA(cudaMemcpy(dql, qlen_eff.data(), 4 * nq, cudaMemcpyHostToDevice));
@@ -977,6 +981,8 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         TPZ_CUDA(cudaEventRecord(ev[4], 0));
         chain_kernel<<<(unsigned)std::min<int64_t>((2 * npos * kChain + 255) / 256, (int64_t)nsm * 64),
                        256>>>(ix->d, sa, o->min_hit_length, dcache, dcprot);
+        count_queued_kernel<<<(unsigned)std::min<int64_t>((2 * npos + 255) / 256, (int64_t)nsm * 8), 256>>>(
+            dcur, 2 * npos, o->min_hit_length, dqueued);
     }
     WalkArgs wa;
     wa.qcat = dq; wa.qoff = dqo; wa.qlen = dql; wa.nq = (int)nq; wa.cursor_base = dcb;
@@ -998,6 +1004,15 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch walk"));
     R->hit_off.assign(nq + 1, 0);
     R->npops.resize(nq); R->ncounted.resize(nq); R->status.resize(nq);
+    {
+        unsigned long long queued = 0;
+        if (cudaMemcpy(&queued, dqueued, sizeof queued, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return bail(tpz::cuda_fail(cudaGetLastError(), "tpz_search_batch counts"));
+        int64_t refills = 0;
+        for (int64_t q = 0; q < nq; ++q) refills += qo[q].refills;
+        R->chain_elems = (int64_t)queued * kChain;
+        R->refill_elems = refills * 32;
+    }
     for (int64_t q = 0; q < nq; ++q) {
         R->hit_off[q + 1] = R->hit_off[q] + qo[q].nhits;
         R->npops[q] = qo[q].npops;
@@ -1144,6 +1159,8 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     r.stage_ms[3] = (tw1.tv_sec - tw0.tv_sec) * 1e3 + (tw1.tv_usec - tw0.tv_usec) / 1e3;
     r.sw_pairs = R->sw_pairs;
     r.sw_cells = R->sw_cells;
+    r.chain_elems = R->chain_elems;
+    r.refill_elems = R->refill_elems;
     *out = &R->r;
     return TPZ_OK;
 }

@@ -43,6 +43,7 @@ struct PopRec {
 struct QueryOut {
     int64_t npops, ncounted;
     int32_t nhits, status;
+    int64_t refills;              // chain caches the walk refilled (32 elements each)
 };
 
 struct SeedArgs {
@@ -93,6 +94,8 @@ __global__ void hsp_batch_kernel(DevIndex ix, const uint8_t *qcat, const int64_t
                                  int32_t *len);
 __global__ void lower_bound_kernel(DevIndex ix, const uint8_t *pcat, const int64_t *poff,
                                    const int32_t *plen, int64_t n, int64_t *out);
+__global__ void count_queued_kernel(const Cursor *cursors, int64_t n, int min_hit_length,
+                                    unsigned long long *count);
 __global__ void sa_search_call_kernel(DevIndex ix, const uint8_t *P, int64_t m, int64_t *out3);
 
 }  // namespace search

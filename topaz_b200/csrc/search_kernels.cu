@@ -264,6 +264,22 @@ __global__ void seed_kernel(DevIndex ix, SeedArgs a) {
     }
 }
 
+// Cursors that enter the queue (the chain kernel computes kChain elements
+// for each): block sums, one atomic per block.
+__global__ void count_queued_kernel(const Cursor *cursors, int64_t n, int min_hit_length,
+                                    unsigned long long *count) {
+    __shared__ unsigned int part;
+    if (threadIdx.x == 0) part = 0;
+    __syncthreads();
+    unsigned int mine = 0;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x)
+        mine += cursors[c].len >= min_hit_length;
+    atomicAdd(&part, mine);
+    __syncthreads();
+    if (threadIdx.x == 0 && part) atomicAdd(count, (unsigned long long)part);
+}
+
 // One thread per pattern: the sa_search idx of a whole pattern.
 __global__ void lower_bound_kernel(DevIndex ix, const uint8_t *pcat, const int64_t *poff,
                                    const int32_t *plen, int64_t n, int64_t *out) {
@@ -502,7 +518,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
     int64_t qsize = 0;
     int nfree = cap + 1, hsize = 0, hmin = kSMax;
     const uint32_t hmask = (uint32_t)a.hash_size - 1;
-    int64_t npops = 0, counter = 0;
+    int64_t npops = 0, counter = 0, refills = 0;
     int status = 0;
     PopRec *trace = a.trace ? a.trace + (int64_t)q * a.trace_cap : nullptr;
     if (lane == 0) {
@@ -544,6 +560,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
         uint32_t elem = 0;
         int32_t eprot = -1;
         if (need) {
+            ++refills;
             // all lanes: the next 32 rows of this cursor
             row = __shfl_sync(0xFFFFFFFFu, row, 0);
             off = __shfl_sync(0xFFFFFFFFu, off, 0);
@@ -690,6 +707,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(DevIndex ix, Walk
         }
         QueryOut qo;
         qo.nhits = n; qo.npops = npops; qo.ncounted = counter; qo.status = status | a.qstatus[q];
+        qo.refills = refills;
         a.qout[q] = qo;
     }
 }

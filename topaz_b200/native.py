@@ -170,7 +170,8 @@ class _SearchResult(ctypes.Structure):
                 ("seed_ms", ctypes.c_double), ("chain_ms", ctypes.c_double),
                 ("positions", ctypes.c_int64), ("qstart", _P32), ("sstart", _P32),
                 ("length", _P32), ("gapopen", _P32), ("mismatch", _P32),
-                ("identity", ctypes.POINTER(ctypes.c_double))]
+                ("identity", ctypes.POINTER(ctypes.c_double)),
+                ("chain_elems", ctypes.c_int64), ("refill_elems", ctypes.c_int64)]
 
 
 def _search_sigs(L):
@@ -301,6 +302,7 @@ class Index:
             out["sw_pairs"], out["sw_cells"] = int(r.sw_pairs), int(r.sw_cells)
             out["seed_ms"], out["chain_ms"] = float(r.seed_ms), float(r.chain_ms)
             out["positions"] = int(r.positions)
+            out["chain_elems"], out["refill_elems"] = int(r.chain_elems), int(r.refill_elems)
             if report is not None:
                 out["bitscore"] = arr(r.bitscore, nh)
                 out["evalue"] = arr(r.evalue, nh)
