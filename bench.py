@@ -485,7 +485,9 @@ def search_bench(args, dev):
         sample = spread(n)
         dt, rr = run(oracle.REF_BIN, sample)
         dt_cli, rm = run(B.CLI, sample)
-        dt_cli_all, _ = run(B.CLI, list(range(len(q_aa))))
+        dt_cli_all, r_all = run(B.CLI, list(range(len(q_aa))))
+        cli_stages = [ln for ln in r_all.stderr.decode(errors="replace").splitlines()
+                      if ln.startswith("timing:")]
         half = len(q_aa) // 2
         out["cpu_reference"] = {"queries_per_s": round(len(sample) / dt, 2), "threads": threads,
                                 "kind": "reference", "sample": "%d queries evenly spaced over the %d "
@@ -512,6 +514,7 @@ def search_bench(args, dev):
         out["cli"] = {"queries_per_s_sample": round(len(sample) / dt_cli, 1),
                       "queries_per_s_all": round(len(q_aa) / dt_cli_all, 1),
                       "sample_s": round(dt_cli, 2), "all_s": round(dt_cli_all, 2),
+                      "stages_all": cli_stages[0] if cli_stages else None,
                       "threads": threads, "api": "topaz search CLI (whole process)"}
         # `topaz index` on the first 100,000 proteins: the reference (host
         # SA-IS) and ours (SA on the device), files compared

@@ -638,14 +638,18 @@ int tpz_index_create(const uint8_t *T, int64_t Tsize, const int64_t *SA, const v
     auto fail = [&](int rc) { tpz_index_destroy(ix); return rc; };
     const int64_t sa_rows = ((Tsize * 8 + 4095) / 4096) * 4096 / 8;
     const int64_t nblocks = (Tsize + 63) / 64;
-    uint8_t *dT; int64_t *dSA, *dps, *dlb; uint32_t *dnl;
+    uint8_t *dT, *dTbase; int64_t *dSA, *dps, *dlb; uint32_t *dnl;
     int rc;
-    if ((rc = dalloc(ix, (void **)&dT, Tsize + 128))) return fail(rc);
+    // 64 bytes in front of the text and 128 behind it: the windows of the
+    // extension kernels read a little past both ends
+    if ((rc = dalloc(ix, (void **)&dTbase, Tsize + 192))) return fail(rc);
+    dT = dTbase + 64;
     if ((rc = dalloc(ix, (void **)&dSA, sa_rows * 8))) return fail(rc);
     if ((rc = dalloc(ix, (void **)&dps, (Psize + 1) * 8))) return fail(rc);
     if ((rc = dalloc(ix, (void **)&dnl, (nblocks + 1) * 4))) return fail(rc);
     if ((rc = dalloc(ix, (void **)&dlb, (kCodes + 1) * 8))) return fail(rc);
-    if (cudaMemset(dT + Tsize, '\n', 128) != cudaSuccess ||
+    if (cudaMemset(dTbase, '\n', 64) != cudaSuccess ||
+        cudaMemset(dT + Tsize, '\n', 128) != cudaSuccess ||
         cudaMemset(dSA + Tsize, 0, (sa_rows - Tsize) * 8) != cudaSuccess ||
         cudaMemcpy(dps, pstart.data(), (Psize + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create copies"));
@@ -750,11 +754,13 @@ int tpz_sa_hsp_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     DevBuf b;
     uint8_t *dq; int64_t *dqo, *drow; int32_t *dql, *dqf, *doff, *dsc, *dln; int8_t *dsub;
     int rc;
-    // + 64: hsp_at's vector loads read up to 15 bytes past a query's end
-    if ((rc = b.alloc(&dq, bytes + 64)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
+    // 64 readable bytes in front of the queries and behind them: hsp_at's
+    // windows read a little past both ends
+    if ((rc = b.alloc(&dq, bytes + 128)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
         (rc = b.alloc(&dqf, n)) || (rc = b.alloc(&doff, n)) || (rc = b.alloc(&drow, n)) ||
         (rc = b.alloc(&dsc, n)) || (rc = b.alloc(&dln, n)) || (rc = b.alloc(&dsub, 625)))
         return rc;
+    dq += 64;
     TPZ_CUDA(cudaMemcpy(dq, qcat, bytes, cudaMemcpyHostToDevice));
     TPZ_CUDA(cudaMemcpy(dqo, qoff, 8 * nq, cudaMemcpyHostToDevice));
     TPZ_CUDA(cudaMemcpy(dql, qlen, 4 * nq, cudaMemcpyHostToDevice));
@@ -938,8 +944,9 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
     Cursor *dcur; Hit *dhits; QueryOut *dqout; PopRec *dtrace = nullptr;
     int32_t *dqnext, *dcprot; uint32_t *dcache;
     int rc;
-    // + 64: hsp_at's vector loads read up to 15 bytes past a query's end
-    if ((rc = b.alloc(&dq, bytes + 64)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
+    // 64 readable bytes in front of the queries and behind them: hsp_at's
+    // windows read a little past both ends
+    if ((rc = b.alloc(&dq, bytes + 128)) || (rc = b.alloc(&dqo, nq)) || (rc = b.alloc(&dql, nq)) ||
         (rc = b.alloc(&dpb, nq + 1)) || (rc = b.alloc(&dcb, nq + 1)) || (rc = b.alloc(&dqs, nq)) ||
         (rc = b.alloc(&dsub, 625)) || (rc = b.alloc(&dcur, 2 * npos + 1)) ||
         (rc = b.alloc(&dscratch, per_q * nq)) || (rc = b.alloc(&dhits, (size_t)nq * max_cap)) ||
@@ -947,6 +954,7 @@ int tpz_search_batch(const tpz_index *ix, const char *qcat, const int64_t *qoff,
         (rc = b.alloc(&dcache, (size_t)kChain * (2 * npos + 1))) ||
         (rc = b.alloc(&dcprot, (size_t)kChain * (2 * npos + 1))))
         return rc;
+    dq += 64;
     if (o->trace_pops > 0 && (rc = b.alloc(&dtrace, (size_t)nq * o->trace_pops))) return rc;
     unsigned long long *dqueued;
     if ((rc = b.alloc(&dqueued, 1))) return rc;

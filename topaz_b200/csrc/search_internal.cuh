@@ -30,6 +30,7 @@ struct Cursor {
 
 constexpr int kWalkWarps = 4;            // queries (warps) per walk block
 constexpr int kChain = 64;               // chain elements cached per cursor
+static_assert(kChain >= 32, "a walk refill stores 32 chain elements in a cursor's cache slot");
 
 struct Hit {
     int32_t protein, gapless_score, gapless_length, suffix_offset;

@@ -89,49 +89,58 @@ __device__ __forceinline__ int64_t protein_of(const DevIndex &ix, int64_t pos) {
     return (int64_t)ix.nl[pos >> 6] + newlines_in_block_before(ix.T, pos);
 }
 
-// Copies bytes [p, p + n) (n <= 64, any alignment) into a thread's 16-byte
-// aligned buffer with aligned 16-byte loads issued together -- one memory
-// round trip for up to 64 bytes instead of one per 8.  Returns the offset of
-// p in the buffer.  The loads may cover up to 15 bytes before p and after
-// p + n: callers keep 16 readable bytes around every window (the text and
-// query buffers are 256-byte aligned and padded at the end).
-__device__ __forceinline__ int stage64(const uint8_t *p, int n, uint4 *buf) {
-    const uintptr_t a = (uintptr_t)p & ~(uintptr_t)15;
-    const int o = (int)((uintptr_t)p - a);
-    const int nv = (o + n + 15) >> 4;
-    const uint4 *src = reinterpret_cast<const uint4 *>(a);
+// 32 bytes of memory from p (any alignment) as 8 words in memory order:
+// nine aligned 4-byte loads issued together, funnel-shifted into place, so
+// the window stays in registers.  Reads up to 3 bytes before p and 35 after
+// it: the text and query buffers keep 64 readable bytes in front of their
+// first byte and behind their last.
+__device__ __forceinline__ void load32(const uint8_t *p, uint32_t (&w)[8]) {
+    const uintptr_t a = (uintptr_t)p & ~(uintptr_t)3;
+    const uint32_t sh = (uint32_t)((uintptr_t)p - a) * 8u;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(a);
+    uint32_t r[9];
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
-        if (k < nv) buf[k] = __ldg(src + k);
-    return o;
+    for (int k = 0; k < 9; ++k) r[k] = __ldg(src + k);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w[k] = __funnelshift_r(r[k], r[k + 1], sh);
+}
+
+// byte k (a compile-time index after unrolling) of a load32 window
+__device__ __forceinline__ uint32_t byte_of(const uint32_t (&w)[8], int k) {
+    return (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;
 }
 
 // sa_hsp (src/search.c:99-190) at text position idx for query offset off.
 // Returns the length (-1 when the first symbols differ; score untouched then).
-// The windows (up to 128 bytes each side) are read 64 bytes at a time with
-// vector loads; the running sums walk them in the reference's order and stop
-// at the first '\n' exactly as its byte loop does.
+// The windows (up to 128 bytes each side) are read 32 bytes per round trip
+// into registers; the running sums walk them in the reference's order and
+// stop at the first '\n' exactly as its byte loop does.
 __device__ int hsp_at(const DevIndex &ix, int64_t idx, const uint8_t *Q, int qlen, int off,
                       const int8_t *sub, int *score) {
     const uint8_t *t = ix.T + idx;
     const uint8_t *q = Q + off;
-    if (t[0] != q[0]) return -1;
-    uint4 tb[5], qb[5];
-    const uint8_t *tc = reinterpret_cast<const uint8_t *>(tb);
-    const uint8_t *qc = reinterpret_cast<const uint8_t *>(qb);
     int64_t mr = ix.Tsize - idx;
     if (mr > qlen - off) mr = qlen - off;
     if (mr > 128) mr = 128;
+    uint32_t tw[8], qw[8];
+    load32(t, tw);
+    load32(q, qw);
+    if ((tw[0] & 0xFFu) != (qw[0] & 0xFFu)) return -1;
     int run = 0, best_r = 0, arg_r = 0;
     bool stop = false;
-    for (int i0 = 0; i0 < (int)mr && !stop; i0 += 64) {
-        const int n = min(64, (int)mr - i0);
-        const int ot = stage64(t + i0, n, tb), oq = stage64(q + i0, n, qb);
-        for (int k = 0; k < n; ++k) {
-            const uint8_t c = tc[ot + k];
-            if (c == '\n') { stop = true; break; }
-            run += sub[(c - 'A') * 25 + (qc[oq + k] - 'A')];
-            if (run >= best_r) { best_r = run; arg_r = i0 + k; }
+    for (int i0 = 0; i0 < (int)mr && !stop; i0 += 32) {
+        if (i0 > 0) { load32(t + i0, tw); load32(q + i0, qw); }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const uint32_t c = byte_of(tw, k);
+            if (!stop && i0 + k < (int)mr) {
+                if (c == '\n') {
+                    stop = true;
+                } else {
+                    run += sub[(c - 'A') * 25 + (byte_of(qw, k) - 'A')];
+                    if (run >= best_r) { best_r = run; arg_r = i0 + k; }
+                }
+            }
         }
     }
     int64_t ml = idx < off ? idx : off;
@@ -139,16 +148,22 @@ __device__ int hsp_at(const DevIndex &ix, int64_t idx, const uint8_t *Q, int qle
     int best_l = 0, arg_l = 0;
     run = 0;
     stop = false;
-    // left: i = 1 .. ml-1 reads t[-i]; a round stages t[-(i0+n-1) .. -i0]
-    for (int i0 = 1; i0 < (int)ml && !stop; i0 += 64) {
-        const int n = min(64, (int)ml - i0);
-        const int ot = stage64(t - (i0 + n - 1), n, tb), oq = stage64(q - (i0 + n - 1), n, qb);
-        for (int k = 0; k < n; ++k) {
-            // byte t[-(i0 + k)] sits at index n - 1 - k of the staged range
-            const uint8_t c = tc[ot + n - 1 - k];
-            if (c == '\n') { stop = true; break; }
-            run += sub[(c - 'A') * 25 + (qc[oq + n - 1 - k] - 'A')];
-            if (run >= best_l) { best_l = run; arg_l = i0 + k; }
+    // left: i = 1 .. ml-1 reads t[-i]; a round loads the 32 bytes that end at
+    // t[-i0], so t[-(i0 + k)] is byte 31 - k
+    for (int i0 = 1; i0 < (int)ml && !stop; i0 += 32) {
+        load32(t - (i0 + 31), tw);
+        load32(q - (i0 + 31), qw);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const uint32_t c = byte_of(tw, 31 - k);
+            if (!stop && i0 + k < (int)ml) {
+                if (c == '\n') {
+                    stop = true;
+                } else {
+                    run += sub[(c - 'A') * 25 + (byte_of(qw, 31 - k) - 'A')];
+                    if (run >= best_l) { best_l = run; arg_l = i0 + k; }
+                }
+            }
         }
     }
     *score = best_l + best_r;

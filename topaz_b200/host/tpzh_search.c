@@ -400,6 +400,7 @@ static void join_init(void) {
 int tpzh_search(const char *fasta, const char *prefix, const tpzh_options *o) {
     struct timeval t0, t1;
     gettimeofday(&t0, NULL);
+    const double t_start = now_s();
     /* the CUDA context comes up while the database files are mapped */
     g_init_started = pthread_create(&g_init_th, NULL, device_init_thread, &g_init_rc) == 0;
     /* db_load / _load_index (src/db.c:34-122) in the same order, with the
@@ -449,7 +450,9 @@ load_fail:
         join_init();
         return -1;
     }
+    const double t_map = now_s();
     join_init();
+    const double init_wait_s = now_s() - t_map;
     if (g_init_rc != 0 && tpz_device_init() != 0) {   /* again here, for this thread's message */
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         return -1;
@@ -519,14 +522,17 @@ load_fail:
     const uint64_t nonzero = c.nonzero, total_hits = c.total_hits;
     fflush(stdout);
     tpzh_fasta_close(&f);
+    const double t_end = now_s();
     tpz_index_destroy(ix);
+    const double destroy_s = now_s() - t_end;
     gettimeofday(&t1, NULL);
     fprintf(stderr, "output %" PRIu64 " hits for %" PRIu64 " queries\n", total_hits, nonzero);
-    fprintf(stderr, "timing: index upload %.2f s, queries %.2f s (%d host threads; summed over "
-            "batches: ingest %.2f s, batch calls %.2f s, format %.2f s; device seed %.0f ms, walk "
-            "%.0f ms, SW + ranking %.0f ms)\n",
-            upload_s, now_s() - t_search, nw, c.ingest_s, c.call_s, c.format_s, c.dev_ms[0],
-            c.dev_ms[1], c.dev_ms[2]);
+    fprintf(stderr, "timing: files mapped %.2f s, device init wait %.2f s, index upload %.2f s, "
+            "queries %.2f s (%d host threads; summed over batches: ingest %.2f s, batch calls "
+            "%.2f s, format %.2f s; device seed %.0f ms, walk %.0f ms, SW + ranking %.0f ms), "
+            "index release %.2f s\n",
+            t_map - t_start, init_wait_s, upload_s, t_end - t_search, nw,
+            c.ingest_s, c.call_s, c.format_s, c.dev_ms[0], c.dev_ms[1], c.dev_ms[2], destroy_s);
     fprintf(stderr, "elapsed time: %.1f seconds\n",
             ((t1.tv_sec - t0.tv_sec) * 1000.0 + (t1.tv_usec - t0.tv_usec) / 1000.0) / 1000);
     fprintf(stderr, "done!\n");
