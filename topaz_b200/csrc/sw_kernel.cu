@@ -262,30 +262,43 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
     }
     uint32_t let1 = ring[(1 - lane) & (kRing - 1)];
 
+    // The row search of a column whose maximum rose runs one step late,
+    // between the next column's diagonal terms and its F / Fm chains: H still
+    // holds the risen column there, and the vote that guards the search then
+    // waits on nothing, so no step stalls on the one before it.
+    bool pend = false;                   // the previous column needs its row found
+    uint32_t pcm = 0u, pthr = 0u;        // its column maximum and threshold
+    int pj = 0;                          // its column
+    auto search = [&]() {
+        if (!a.score_only && __any_sync(0xFFFFFFFFu, pend)) {
+            // smallest row holding the column maximum, both halves at once:
+            // max(H - cm, -1) is 0 on rows holding it and -1 elsewhere; those
+            // rows contribute R - r and the largest contribution wins
+            const uint32_t negv = __viaddmax_s16x2(~pcm, 0x00010001u, NEGINF);
+            uint32_t acc = 0u;
+#pragma unroll
+            for (int r = 0; r < R; r += 2) {
+                const uint32_t g0 =
+                    ~__viaddmax_s16x2(H[r], negv, 0xFFFFFFFFu) & pack2(R - r, R - r);
+                if (r + 1 < R) {
+                    const uint32_t g1 = ~__viaddmax_s16x2(H[r + 1], negv, 0xFFFFFFFFu) &
+                                        pack2(R - r - 1, R - r - 1);
+                    acc = __vimax3_s16x2(acc, g0, g1);
+                } else {
+                    acc = __vimax_s16x2_relu(acc, g0);
+                }
+            }
+            if (pend) {
+                if (lo16(pcm) > lo16(pthr)) { colA = pj; rowA = i0 + R - lo16(acc); }
+                if (hi16(pcm) > hi16(pthr)) { colB = pj; rowB = i0 + R - hi16(acc); }
+            }
+        }
+        pend = false;
+    };
+
     auto step = [&](const int k, const uint32_t (&cwa)[W], const uint32_t (&cwb)[W],
                     uint32_t (&nwa)[W], uint32_t (&nwb)[W]) {
         const int j = k - lane;
-        if ((k & 31) == 0 && k > 0) {
-            ring[(k + 32 + lane) & (kRing - 1)] = (uint16_t)pre;
-            pre = letter_pair(a, sA, slA, sB, slB, k + 64 + lane);
-            // warp maximum so far: a lane's rise below it cannot end up as
-            // the alignment's maximum, so it needs no row search
-            uint32_t wm = runmax;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                wm = __vimax_s16x2_relu(wm, __shfl_xor_sync(0xFFFFFFFFu, wm, o));
-            if (TPZ_LANES == 16) {
-                // u8 pass: a pair whose maximum reached 255 - bias is decided
-                // (the i16 pass reruns it), so it needs no more row searches,
-                // and a task whose pairs are both decided stops here
-                const bool da = lo16(wm) + a.bias >= 255, db = hi16(wm) + a.bias >= 255;
-                if (da) wm = (wm & 0xFFFF0000u) | 0x7FFFu;
-                if (db) wm = (wm & 0x0000FFFFu) | 0x7FFF0000u;
-                if (da && (db || pB < 0)) decided = true;
-            }
-            wmax = wm;
-            __syncwarp();
-        }
         uint32_t inH = __shfl_up_sync(0xFFFFFFFFu, outH, 1);
         uint32_t inF = __shfl_up_sync(0xFFFFFFFFu, outF, 1);
         uint32_t inFm = __shfl_up_sync(0xFFFFFFFFu, outFm, 1);
@@ -304,84 +317,93 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             nwb[w] = profB[((let1 >> 8) * W + w) * 32 + lane];
         }
         let1 = ring[(j + 2) & (kRing - 1)];
-        bool need = false;
-        uint32_t cmx = 0u, thr = 0u;
-        if (j >= 0 && j < N) {
-            uint32_t F = inF, Fm = inFm, D = diag;
-            // first every row's diagonal term and its gap-open candidate (they
-            // depend only on the previous column), then the F / Fm chains,
-            // the only row-to-row dependences, with E and H hanging off them
-            uint32_t Xa[R], Xga[R];
+        // every lane computes every step: a lane before its first column
+        // (j < 0) sees pad letters and zero inputs, so its H stays 0 and its
+        // E only goes negative, which no later cell can see through the
+        // relu; past the subject's end (j >= N) the pad columns only hold
+        // values below a real cell's, which can never be the maximum
+        uint32_t F = inF, Fm = inFm, D = diag;
+        // first every row's diagonal term and its gap-open candidate (they
+        // depend only on the previous column), then the F / Fm chains, the
+        // only row-to-row dependences, with E and H hanging off them
+        uint32_t Xa[R], Xga[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t sc = prmt(cwa[r >> 2], cwb[r >> 2], SEL[r & 3]);
-                Xa[r] = __viaddmax_s16x2_relu(r == 0 ? D : H[r - 1], sc, E[r]);
-                Xga[r] = __viaddmax_s16x2(Xa[r], NGO, NEGINF);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t Hn = __vimax_s16x2_relu(Xa[r], F);
-                const uint32_t Gp = __viaddmax_s16x2(Fm, ngo[r], Xga[r]);
-                E[r] = __viaddmax_s16x2(E[r], NGE, Gp);
-                F = __viaddmax_s16x2(F, NGE, Xga[r]);
-                Fm = __viaddmax_s16x2(Fm, nge[r], Xga[r]);
-                H[r] = Hn;
-            }
-            // column maximum of the lane's rows, floored at the search
-            // threshold max(running max, warp maximum - 1): a half needs its
-            // row found when it rises above the threshold, i.e. above the
-            // lane's running max and not below the warp maximum of the last
-            // refresh (anything lower cannot be the alignment maximum).  The
-            // running max may so take the value warp maximum - 1 without a
-            // cell holding it; such a lane can never hold the final maximum.
-            thr = __viaddmax_s16x2(wmax, 0xFFFFFFFFu, runmax);
-            uint32_t cm = thr;
-#pragma unroll
-            for (int r = 0; r + 1 < R; r += 2) cm = __vimax3_s16x2(cm, H[r], H[r + 1]);
-            if (R & 1) cm = __vimax_s16x2_relu(cm, H[R - 1]);
-            outH = H[R - 1];
-            outF = F;
-            outFm = Fm;
-            if (MULTI && lane == 31 && st + 1 < stripes) {
-                uint32_t *b = bnd + 3 * (size_t)j;
-                b[0] = outH; b[1] = outF; b[2] = outFm;
-            }
-            need = cm != thr;
-            runmax = cm;
-            cmx = cm;
+        for (int r = 0; r < R; ++r) {
+            const uint32_t sc = prmt(cwa[r >> 2], cwb[r >> 2], SEL[r & 3]);
+            Xa[r] = __viaddmax_s16x2_relu(r == 0 ? D : H[r - 1], sc, E[r]);
+            Xga[r] = __viaddmax_s16x2(Xa[r], NGO, NEGINF);
         }
-        if (!a.score_only && __any_sync(0xFFFFFFFFu, need)) {
-            // smallest row holding the column maximum, both halves at once:
-            // max(H - cm, -1) is 0 on rows holding it and -1 elsewhere; those
-            // rows contribute R - r and the largest contribution wins
-            const uint32_t negv = __viaddmax_s16x2(~cmx, 0x00010001u, NEGINF);
-            uint32_t acc = 0u;
+        search();
 #pragma unroll
-            for (int r = 0; r < R; r += 2) {
-                const uint32_t g0 =
-                    ~__viaddmax_s16x2(H[r], negv, 0xFFFFFFFFu) & pack2(R - r, R - r);
-                if (r + 1 < R) {
-                    const uint32_t g1 = ~__viaddmax_s16x2(H[r + 1], negv, 0xFFFFFFFFu) &
-                                        pack2(R - r - 1, R - r - 1);
-                    acc = __vimax3_s16x2(acc, g0, g1);
-                } else {
-                    acc = __vimax_s16x2_relu(acc, g0);
-                }
-            }
-            if (need) {
-                if (lo16(cmx) > lo16(thr)) { colA = j; rowA = i0 + R - lo16(acc); }
-                if (hi16(cmx) > hi16(thr)) { colB = j; rowB = i0 + R - hi16(acc); }
-            }
+        for (int r = 0; r < R; ++r) {
+            const uint32_t Hn = __vimax_s16x2_relu(Xa[r], F);
+            const uint32_t Gp = __viaddmax_s16x2(Fm, ngo[r], Xga[r]);
+            E[r] = __viaddmax_s16x2(E[r], NGE, Gp);
+            F = __viaddmax_s16x2(F, NGE, Xga[r]);
+            Fm = __viaddmax_s16x2(Fm, nge[r], Xga[r]);
+            H[r] = Hn;
         }
+        // column maximum of the lane's rows, floored at the search threshold
+        // max(running max, warp maximum - 1): a half needs its row found when
+        // it rises above the threshold, i.e. above the lane's running max and
+        // not below the warp maximum of the last refresh (anything lower
+        // cannot be the alignment maximum).  The running max may so take the
+        // value warp maximum - 1 without a cell holding it; such a lane can
+        // never hold the final maximum.
+        const uint32_t thr = __viaddmax_s16x2(wmax, 0xFFFFFFFFu, runmax);
+        uint32_t cm = thr;
+#pragma unroll
+        for (int r = 0; r + 1 < R; r += 2) cm = __vimax3_s16x2(cm, H[r], H[r + 1]);
+        if (R & 1) cm = __vimax_s16x2_relu(cm, H[R - 1]);
+        outH = H[R - 1];
+        outF = F;
+        outFm = Fm;
+        if (MULTI && lane == 31 && st + 1 < stripes && j >= 0 && j < N) {
+            uint32_t *b = bnd + 3 * (size_t)j;
+            b[0] = outH; b[1] = outF; b[2] = outFm;
+        }
+        pend = cm != thr;
+        pcm = cm;
+        pthr = thr;
+        pj = j;
+        runmax = cm;
         diag = inH;
     };
     uint32_t wa2[W], wb2[W];
     // an even step count; a step past N + 30 finds every lane past the end
     const int steps = (N + 32) & ~1;
-    for (int k = 0; k < steps && !decided; k += 2) {
-        step(k, wa, wb, wa2, wb2);
-        step(k + 1, wa2, wb2, wa, wb);
+    for (int k0 = 0; k0 < steps; k0 += 32) {
+        if (k0 > 0) {
+            // every 32 steps the lanes store the next 32 columns' letters and
+            // fetch 32 more
+            ring[(k0 + 32 + lane) & (kRing - 1)] = (uint16_t)pre;
+            pre = letter_pair(a, sA, slA, sB, slB, k0 + 64 + lane);
+            // warp maximum so far: a lane's rise below it cannot end up as
+            // the alignment's maximum, so it needs no row search
+            uint32_t wm = runmax;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                wm = __vimax_s16x2_relu(wm, __shfl_xor_sync(0xFFFFFFFFu, wm, o));
+            if (TPZ_LANES == 16) {
+                // u8 pass: a pair whose maximum reached 255 - bias is decided
+                // (the i16 pass reruns it), so it needs no more row searches,
+                // and a task whose pairs are both decided stops here
+                const bool da = lo16(wm) + a.bias >= 255, db = hi16(wm) + a.bias >= 255;
+                if (da) wm = (wm & 0xFFFF0000u) | 0x7FFFu;
+                if (db) wm = (wm & 0x0000FFFFu) | 0x7FFF0000u;
+                if (da && (db || pB < 0)) decided = true;
+            }
+            wmax = wm;
+            __syncwarp();
+            if (decided) break;
+        }
+        const int kend = min(k0 + 32, steps);
+        for (int k = k0; k < kend; k += 2) {
+            step(k, wa, wb, wa2, wb2);
+            step(k + 1, wa2, wb2, wa, wb);
+        }
     }
+    search();                           // the last column's, if it rose
 
     if (a.score_only || decided) { colA = colB = 0; rowA = rowB = 0; }
     kA = max(kA, best_key(lo16(runmax), colA, rowA));
@@ -1371,20 +1393,23 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         return TPZ_E_ARG;
     }
     if (n == 0) return TPZ_OK;
-    // Pairs go in two chunks when there are many: the first sixteenth, then
-    // the rest.  The first chunk's kernels run while the rest is copied in, and
-    // the two chunks run on separate streams (lanes), so the second chunk's
-    // kernels fill the GPU while the first chunk's last tasks finish; each
-    // chunk's results are copied out as soon as they are done.
-    int64_t cut[3] = {0, n, n};
+    // Pairs go in up to four chunks of 1/64, 4/64, 16/64 and 43/64 of the
+    // batch: the copy in of the inputs runs about six times faster than the
+    // kernels, so each chunk's inputs arrive while the chunk before it
+    // computes and the GPU waits only for the first 1/64.  Consecutive chunks
+    // run on alternating streams (lanes), so a chunk's kernels fill the GPU
+    // while the previous chunk's last tasks finish; each chunk's results are
+    // copied out as soon as they are done.
+    constexpr int kMaxChunks = 4;
+    int64_t cut[kMaxChunks + 1] = {0, n};
     int nch = 1;
     if (n >= 65536) {
-        cut[1] = n / 16; cut[2] = n;
-        nch = 2;
+        cut[1] = n / 64; cut[2] = 5 * (n / 64); cut[3] = 21 * (n / 64); cut[4] = n;
+        nch = 4;
     }
     // host-side validation and the byte ranges each chunk reads, chunks
     // scanned on their own threads
-    Span sp[2];
+    Span sp[kMaxChunks];
     {
         std::vector<std::thread> th;
         for (int c = 1; c < nch; ++c)
@@ -1445,7 +1470,8 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         }
         return e;
     };
-    cudaEvent_t *in_ready = g_hb.ev, *done = g_hb.ev + 2;
+    static_assert(2 * kMaxChunks <= (int)(sizeof g_hb.ev / sizeof g_hb.ev[0]), "events per chunk");
+    cudaEvent_t *in_ready = g_hb.ev, *done = g_hb.ev + kMaxChunks;
     for (int c = 0; c < nch; ++c) {
         const int64_t a = cut[c], m = cut[c + 1] - cut[c];
         TPZ_CUDA(copy_new(q, dq, sp[c].qlo, sp[c].qhi, qc_lo, qc_hi));
@@ -1458,12 +1484,12 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
     }
     for (int c = 0; c < nch; ++c) {
         const int64_t a = cut[c], m = cut[c + 1] - cut[c];
-        cudaStream_t cs = cst[c];
+        cudaStream_t cs = cst[c & 1];
         TPZ_CUDA(cudaStreamWaitEvent(cs, in_ready[c], 0));
         rc = tpz::sw::batch_device_x(m, dq, dqoff + a, dqlen + a, ds, dsoff + a, dslen + a,
                                      mat625, gap_open, gap_extend, dsc + a, dre + a, drd + a,
                                      dst + a, cs, nullptr, nullptr, 0, nullptr, 0,
-                                     sp[c].multi_maxn, c);
+                                     sp[c].multi_maxn, c & 1);
         if (rc) {
             cudaStreamSynchronize(hs);
             cudaStreamSynchronize(cst[0]);

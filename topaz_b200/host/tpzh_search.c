@@ -76,6 +76,53 @@ static int map_file(const char *prefix, const char *ext, map_t *m) {
     return 0;
 }
 
+/* Page-table prefault of the text and SA mappings: threads touch one byte
+ * per page while the CUDA context comes up, so the index upload that follows
+ * copies from mapped pages instead of taking a fault per 4 KB page. */
+#define TPZH_PREFAULT_THREADS 8
+typedef struct {
+    const volatile uint8_t *p;
+    uint64_t n;
+    uint64_t sum;
+} prefault_t;
+
+static void *prefault_thread(void *arg) {
+    prefault_t *a = (prefault_t *)arg;
+    uint64_t s = 0;
+    for (uint64_t i = 0; i < a->n; i += 4096) s += a->p[i];
+    a->sum = s;
+    return NULL;
+}
+
+typedef struct {
+    pthread_t th[2 * TPZH_PREFAULT_THREADS];
+    prefault_t part[2 * TPZH_PREFAULT_THREADS];
+    int started[2 * TPZH_PREFAULT_THREADS];
+} prefault_set_t;
+
+static void prefault_start(prefault_set_t *ps, const map_t *a, const map_t *b) {
+    memset(ps, 0, sizeof *ps);
+    const map_t *m[2] = {a, b};
+    for (int f = 0; f < 2; ++f) {
+        const uint64_t n = m[f]->size;
+        const uint64_t chunk = ((n / TPZH_PREFAULT_THREADS) + 4095) & ~(uint64_t)4095;
+        for (int t = 0; t < TPZH_PREFAULT_THREADS; ++t) {
+            const uint64_t lo = (uint64_t)t * chunk;
+            if (!chunk || lo >= n) break;
+            const int k = f * TPZH_PREFAULT_THREADS + t;
+            ps->part[k].p = (const volatile uint8_t *)m[f]->data + lo;
+            ps->part[k].n = n - lo < chunk ? n - lo : chunk;
+            ps->started[k] = pthread_create(&ps->th[k], NULL, prefault_thread, &ps->part[k]) == 0;
+        }
+    }
+}
+
+static void prefault_join(prefault_set_t *ps) {
+    for (int k = 0; k < 2 * TPZH_PREFAULT_THREADS; ++k)
+        if (ps->started[k]) pthread_join(ps->th[k], NULL);
+    memset(ps->started, 0, sizeof ps->started);
+}
+
 typedef struct {
     int64_t idx;
     double bits, evalue;
@@ -451,8 +498,12 @@ load_fail:
         return -1;
     }
     const double t_map = now_s();
+    prefault_set_t pf;
+    prefault_start(&pf, &T, &SA);
     join_init();
     const double init_wait_s = now_s() - t_map;
+    prefault_join(&pf);
+    const double prefault_wait_s = now_s() - t_map - init_wait_s;
     if (g_init_rc != 0 && tpz_device_init() != 0) {   /* again here, for this thread's message */
         fprintf(stderr, "Error: %s\n", tpz_last_error());
         return -1;
@@ -527,11 +578,11 @@ load_fail:
     const double destroy_s = now_s() - t_end;
     gettimeofday(&t1, NULL);
     fprintf(stderr, "output %" PRIu64 " hits for %" PRIu64 " queries\n", total_hits, nonzero);
-    fprintf(stderr, "timing: files mapped %.2f s, device init wait %.2f s, index upload %.2f s, "
-            "queries %.2f s (%d host threads; summed over batches: ingest %.2f s, batch calls "
-            "%.2f s, format %.2f s; device seed %.0f ms, walk %.0f ms, SW + ranking %.0f ms), "
-            "index release %.2f s\n",
-            t_map - t_start, init_wait_s, upload_s, t_end - t_search, nw,
+    fprintf(stderr, "timing: files mapped %.2f s, device init wait %.2f s, page prefault wait "
+            "%.2f s, index upload %.2f s, queries %.2f s (%d host threads; summed over batches: "
+            "ingest %.2f s, batch calls %.2f s, format %.2f s; device seed %.0f ms, walk %.0f ms, "
+            "SW + ranking %.0f ms), index release %.2f s\n",
+            t_map - t_start, init_wait_s, prefault_wait_s, upload_s, t_end - t_search, nw,
             c.ingest_s, c.call_s, c.format_s, c.dev_ms[0], c.dev_ms[1], c.dev_ms[2], destroy_s);
     fprintf(stderr, "elapsed time: %.1f seconds\n",
             ((t1.tv_sec - t0.tv_sec) * 1000.0 + (t1.tv_usec - t0.tv_usec) / 1000.0) / 1000);
