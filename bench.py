@@ -264,13 +264,40 @@ def extension_roofline(chain_elems, chain_ms, refill_elems, pops):
             "l2_hit_rate": "profiles/search_kernels_small.md (ncu)"}
 
 
+_HBM_LIVE = []
+
+
 def measured_hbm_gbs():
-    """(peak GB/s, where it comes from)"""
+    """(peak GB/s, where it comes from): MEASURED_PEAKS.json when present, else a
+    device-to-device copy of 2 GiB timed here (bytes read + written), else the
+    fallback figure"""
     try:
         return (float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]),
                 "measured: MEASURED_PEAKS.json hbm_gbs (copy)")
     except (OSError, KeyError, ValueError):
-        return 6650.0, "fallback: 6.65 TB/s, an earlier copy measurement on this pool"
+        pass
+    if not _HBM_LIVE:
+        try:
+            import torch
+            n = 1 << 31
+            a = torch.empty(n, dtype=torch.uint8, device="cuda")
+            b = torch.empty(n, dtype=torch.uint8, device="cuda")
+            for _ in range(2):
+                b.copy_(a)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                b.copy_(a)
+            e1.record()
+            torch.cuda.synchronize()
+            _HBM_LIVE.append(2 * n * 5 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+            del a, b
+            torch.cuda.empty_cache()
+        except Exception:                  # no device: the fallback below
+            _HBM_LIVE.append(None)
+    if _HBM_LIVE[0]:
+        return round(_HBM_LIVE[0], 1), "measured live: 2 GiB device-to-device copy (read + write bytes)"
+    return 6650.0, "fallback: 6.65 TB/s, an earlier copy measurement on this pool"
 
 
 def large_bench(args, dev):
