@@ -98,6 +98,13 @@ struct Args {
     int32_t *next_task;      // per R bin task counter
     int32_t *rerun;          // pairs that need the i16 lane length
     int32_t *rerun_count;
+    // per row bin (null: one list for all bins): the u8 pass of bin b appends
+    // its saturated pairs at rerun + rinfo[2b] and counts them here, so the
+    // i16 pass of the bin can follow it on the same stream
+    int32_t *rerun_bin_count;
+    // null: a bin's pairs are sorted[rinfo[2b] ..] and number rinfo[2b + 1];
+    // else the count is task_count[b] (the i16 pass over a bin's rerun list)
+    const int32_t *task_count;
     int ssw_lanes;           // 16 (u8 pass) or 8 (i16 pass)
     int gap_open, gap_extend, bias;
     int translate;           // 1: q/s bytes go through xq/xs first
@@ -142,10 +149,11 @@ __device__ __forceinline__ uint32_t letter_pair(const Args &a, const int8_t *sA,
 }
 
 // One task: pairs pA and pB (pB < 0: none) in the halves of the int16x2
-// lanes.  The pass (16 SSW lanes = u8, 8 = i16) and the list that saturated
-// u8 results go to come from `a` (QM = false) or, for the query-major
-// kernel, from qm_lanes / qm_rerun / qm_rerun_count; QM = true also means
-// that profA/profB already hold the query profile (both pairs share it).
+// lanes.  The pass (16 SSW lanes = u8, 8 = i16) comes from `a` (QM = false)
+// or, for the query-major kernel, from qm_lanes; saturated u8 results go to
+// qm_rerun / qm_rerun_count when given, else to a.rerun / a.rerun_count.
+// QM = true also means that profA/profB already hold the query profile
+// (both pairs share it).
 template <int R, bool MULTI, bool QM = false>
 __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
                                          uint32_t *profA, uint32_t *profB, uint16_t *ring,
@@ -427,8 +435,8 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             const int row = key ? 0xFFFF - (int)(key & 0xFFFF) : 0;
             if (TPZ_LANES == 16 && v + a.bias >= 255) {
                 // u8 pass saturated: the i16 pass decides (src/ssw.c:863-865)
-                int32_t *rr = QM ? qm_rerun : a.rerun;
-                const int slot = atomicAdd(QM ? qm_rerun_count : a.rerun_count, 1);
+                int32_t *rr = qm_rerun ? qm_rerun : a.rerun;
+                const int slot = atomicAdd(qm_rerun ? qm_rerun_count : a.rerun_count, 1);
                 rr[slot] = p;
             } else if (TPZ_LANES == 8 && a.exact_list && v >= a.exact_threshold) {
                 // near the i16 limit: 16-bit lanes may wrap, redo in 32 bits
@@ -456,9 +464,11 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
     uint16_t *ring = reinterpret_cast<uint16_t *>(profB + profile_bytes(R) / 4);
     const int lane = threadIdx.x;
     const int start = a.rinfo[2 * bin];
-    const int count = a.rinfo[2 * bin + 1];
+    const int count = a.task_count ? a.task_count[bin] : a.rinfo[2 * bin + 1];
     const int ntask = (count + 1) / 2;
     if (ntask == 0) return;
+    int32_t *rr_list = a.rerun_bin_count ? a.rerun + start : nullptr;
+    int32_t *rr_count = a.rerun_bin_count ? a.rerun_bin_count + bin : nullptr;
 
     for (int i = lane; i < 26 * kMatStride; i += 32) {
         const int r = i / kMatStride, c = i % kMatStride;
@@ -475,11 +485,12 @@ __global__ void __launch_bounds__(32) sw_bin_kernel(const __grid_constant__ Args
         if constexpr (R == kMaxR) {
             if (stripes > 1) {
                 run_task<R, true>(a, pA, pB, smat, profA, profB, ring, stripes,
-                                  a.bnd + (size_t)blockIdx.x * a.bnd_words);
+                                  a.bnd + (size_t)blockIdx.x * a.bnd_words, 0, rr_list,
+                                  rr_count);
                 continue;
             }
         }
-        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr);
+        run_task<R, false>(a, pA, pB, smat, profA, profB, ring, 1, nullptr, 0, rr_list, rr_count);
     }
 }
 
@@ -765,7 +776,7 @@ struct Table<0> {
     static void fill(KernelFn *) {}
 };
 
-constexpr int kAuxStreams = 4;
+constexpr int kAuxStreams = 8;
 
 struct LaunchCfg {
     KernelFn fn[kMaxR];
@@ -837,10 +848,14 @@ __host__ __device__ constexpr int bin_rows(int b) { return b < kMaxR ? b + 1 : k
 __host__ __device__ constexpr int bin_stripes(int b) { return b < kMaxR ? 1 : b - 30; }
 constexpr int kUsedRBins = kMaxR + kMaxStripes - 1;     // 39
 
+// One pass over the pairs (all of them, or list[0 .. *list_n)): counting sort
+// into row bins, then one persistent kernel per bin.  With a16, each bin's
+// kernel is followed on its stream by the i16 pass over the pairs of that bin
+// that saturated, so no pass waits for the whole batch.
 static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t *list,
                         const int32_t *list_n, int32_t *counts, int32_t *cursor, int32_t *sorted,
                         int32_t *multi_maxn, cudaStream_t st, int64_t &launches,
-                        int *host_maxn, int known_maxn = -1) {
+                        int *host_maxn, int known_maxn = -1, Args *a16 = nullptr) {
     const int nsm = sm_count();
     TPZ_CUDA(cudaMemsetAsync(counts, 0, sizeof(int32_t) * kBins, st));
     const int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
@@ -867,6 +882,7 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
             TPZ_CUDA(cudaMallocAsync((void **)&a.bnd, bytes, st));
         }
     }
+    if (a16) { a16->bnd = a.bnd; a16->bnd_words = a.bnd_words; }
     // one persistent kernel per row bin, longest rows first, spread over the
     // auxiliary streams so that each kernel's tail overlaps the next one;
     // the multi-stripe bins share one boundary buffer and stay on aux[0]
@@ -880,6 +896,10 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
         cudaStream_t xs = S > 1 ? cfg->aux[0] : cfg->aux[rr++ % kAuxStreams];
         cfg->fn[R - 1]<<<grid, 32, cfg->smem[R - 1], xs>>>(a, b, S);
         ++launches;
+        if (a16) {
+            cfg->fn[R - 1]<<<grid, 32, cfg->smem[R - 1], xs>>>(*a16, b, S);
+            ++launches;
+        }
     }
     for (int i = 0; i < kAuxStreams; ++i) {
         TPZ_CUDA(cudaEventRecord(cfg->join[i], cfg->aux[i]));
@@ -962,8 +982,9 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     if (rc) return rc;
 
     // workspace: counts, cursor, rinfo, next_task, rerun_count, multi_maxn,
-    // exact_count | sorted, rerun, exact_list
-    const size_t small = sizeof(int32_t) * (2 * kBins + 2 * kRBins + kRBins + 8);
+    // exact_count, (n_sub), per-bin rerun counts, i16 task counters | sorted,
+    // rerun, exact_list
+    const size_t small = sizeof(int32_t) * (2 * kBins + 2 * kRBins + kRBins + 8 + 2 * kRBins);
     const size_t bytes = small + sizeof(int32_t) * 3 * (size_t)n;
     char *ws = nullptr;
     TPZ_CUDA(cudaMallocAsync((void **)&ws, bytes, st));
@@ -974,6 +995,8 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     int32_t *rerun_count = next_task + kRBins;
     int32_t *multi_maxn = rerun_count + 1;
     int32_t *exact_count = rerun_count + 2;
+    int32_t *rerun_bin_count = rerun_count + 8;
+    int32_t *next_task16 = rerun_bin_count + kRBins;
     int32_t *sorted = (int32_t *)(ws + small);
     int32_t *rerun = sorted + n;
     int32_t *exact_list = rerun + n;
@@ -1001,25 +1024,30 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     a.exact_list = exact_list;
     a.exact_count = exact_count;
     a.exact_threshold = std::min(32767 - 2 * std::max(mx, 1), kBig);
+    a.rerun_bin_count = rerun_bin_count;
+    a.task_count = nullptr;
+    // the i16 pass of a bin: its saturated pairs, in the bin's slice of rerun
+    Args a16 = a;
+    a16.ssw_lanes = 8;
+    a16.sorted = rerun;
+    a16.task_count = rerun_bin_count;
+    a16.next_task = next_task16;
+    a16.rerun_bin_count = nullptr;
 
     int64_t launches = 0;
     int host_maxn = 0;
-    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, 4 * sizeof(int32_t), st));
+    TPZ_CUDA(cudaMemsetAsync(rerun_count, 0, (8 + 2 * kRBins) * sizeof(int32_t), st));
     a.ssw_lanes = 16;
     if (subset) {
         // the first round over the given pair ids only
         int32_t *d_nsub = rerun_count + 3;
         set_i32_kernel<<<1, 1, 0, st>>>(d_nsub, (int32_t)nsub);
         rc = launch_round(cfg, a, nsub, subset, d_nsub, counts, cursor, sorted, multi_maxn, st,
-                          launches, &host_maxn);
+                          launches, &host_maxn, -1, &a16);
     } else {
         rc = launch_round(cfg, a, n, nullptr, nullptr, counts, cursor, sorted, multi_maxn, st,
-                          launches, &host_maxn, known_multi_maxn);
+                          launches, &host_maxn, known_multi_maxn, &a16);
     }
-    if (rc) { if (a.bnd) cudaFreeAsync(a.bnd, st); cudaFreeAsync(ws, st); return rc; }
-    a.ssw_lanes = 8;
-    rc = launch_round(cfg, a, n, rerun, rerun_count, counts, cursor, sorted, multi_maxn, st,
-                      launches, nullptr);
     if (rc == TPZ_OK && (host_maxn > 0 || (int64_t)kStripeRows * mx >= a.exact_threshold)) {
         // only queries longer than one stripe, or matrices with large
         // entries, can come near the 16-bit limit
@@ -1176,6 +1204,8 @@ int batch_device_grouped(int64_t n, const int8_t *q, const int64_t *qoff, const 
         return cuda_fail(cudaGetLastError(), "batch_device_grouped copies");
     }
     Args a;
+    a.rerun_bin_count = nullptr;
+    a.task_count = nullptr;
     memset(&a, 0, sizeof a);
     a.q = q; a.qoff = qoff; a.qlen = qlen; a.s = s; a.soff = soff; a.slen = slen;
     a.score = score; a.ref_end = ref_end; a.read_end = read_end; a.status = status;
@@ -1393,19 +1423,20 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         return TPZ_E_ARG;
     }
     if (n == 0) return TPZ_OK;
-    // Pairs go in up to four chunks of 1/64, 4/64, 16/64 and 43/64 of the
-    // batch: the copy in of the inputs runs about six times faster than the
-    // kernels, so each chunk's inputs arrive while the chunk before it
-    // computes and the GPU waits only for the first 1/64.  Consecutive chunks
-    // run on alternating streams (lanes), so a chunk's kernels fill the GPU
-    // while the previous chunk's last tasks finish; each chunk's results are
-    // copied out as soon as they are done.
+    // Pairs go in three chunks of 1/16, 3/16 and 12/16 of the batch: the copy
+    // in of the inputs runs about six times faster than the kernels, so each
+    // chunk's inputs arrive while the chunk before it computes and the GPU
+    // waits only for the first sixteenth.  Consecutive chunks run on
+    // alternating streams (lanes), so a chunk's kernels fill the GPU while
+    // the previous chunk's last tasks finish; each chunk's results are
+    // copied out as soon as they are done.  (Four chunks from 1/64 measured
+    // 3 % slower: a small chunk still pays its longest task twice.)
     constexpr int kMaxChunks = 4;
     int64_t cut[kMaxChunks + 1] = {0, n};
     int nch = 1;
     if (n >= 65536) {
-        cut[1] = n / 64; cut[2] = 5 * (n / 64); cut[3] = 21 * (n / 64); cut[4] = n;
-        nch = 4;
+        cut[1] = n / 16; cut[2] = 4 * (n / 16); cut[3] = n;
+        nch = 3;
     }
     // host-side validation and the byte ranges each chunk reads, chunks
     // scanned on their own threads
@@ -1534,6 +1565,8 @@ int tpz_sw_align_one(const int8_t *q, int32_t qlen, const int8_t *s, int32_t sle
         return TPZ_E_ARG;
     }
     Args a;
+    a.rerun_bin_count = nullptr;
+    a.task_count = nullptr;
     memset(&a, 0, sizeof a);
     a.q = q; a.s = s;
     a.score = out4; a.ref_end = out4 + 1; a.read_end = out4 + 2; a.status = out4 + 3;
@@ -1708,6 +1741,8 @@ extern "C" int tpz_sw_batch_device_noalloc(int64_t n, const int8_t *q, const int
     int32_t *rerun = sorted + kNoAllocMaxPairs;
 
     Args a;
+    a.rerun_bin_count = nullptr;
+    a.task_count = nullptr;
     a.q = q; a.qoff = qoff; a.qlen = qlen; a.s = s; a.soff = soff; a.slen = slen;
     a.score = score; a.ref_end = ref_end; a.read_end = read_end; a.status = status;
     a.sorted = sorted; a.rinfo = rinfo; a.next_task = next_task;
