@@ -59,18 +59,9 @@ int dalloc(tpz_index *ix, void **p, size_t bytes) {
 // Per-call device buffers, stream-ordered on the calling thread's default
 // stream (the library is built with per-thread default streams), so calls
 // from different host threads neither wait for each other's allocations nor
-// for each other's kernels.  The pool keeps freed memory for the next call.
-void keep_pool_memory() {
-    static thread_local int done_dev = -1;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev == done_dev) return;
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    done_dev = dev;
-}
+// for each other's kernels.  The pool keeps freed memory for the next call
+// (tpz::keep_pool_memory).
+using tpz::keep_pool_memory;
 
 struct DevBuf {
     std::vector<void *> ptrs;

@@ -980,6 +980,7 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
     const LaunchCfg *cfg = nullptr;
     int rc = launch_cfg(&cfg, lane);
     if (rc) return rc;
+    keep_pool_memory();
 
     // workspace: counts, cursor, rinfo, next_task, rerun_count, multi_maxn,
     // exact_count, (n_sub), per-bin rerun counts, i16 task counters | sorted,

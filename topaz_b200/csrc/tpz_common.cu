@@ -66,6 +66,18 @@ int matrix_by_name(const char *name, int8_t *out625) {
     return TPZ_E_ARG;
 }
 
+void keep_pool_memory() {
+    static thread_local int done_dev = -1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev == done_dev) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done_dev = dev;
+}
+
 int sm_count() {
     static std::mutex mu;
     static std::vector<int> cache;

@@ -28,6 +28,12 @@ int matrix_by_name(const char *name, int8_t *out625);
 // SMs of the current device (cached per device).
 int sm_count();
 
+// Sets the current device's default memory pool to keep freed memory
+// instead of returning it at every synchronization, so the stream-ordered
+// per-call buffers are reused rather than mapped again (once per thread and
+// device).
+void keep_pool_memory();
+
 // Inline PTX byte permute, including the sign-replicate selector bit that
 // the generic prmt form supports (bit 3 of each selector nibble).
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
