@@ -784,6 +784,8 @@ struct LaunchCfg {
     int blocks_per_sm[kMaxR];
     cudaStream_t aux[kAuxStreams];       // bin kernels overlap their tails here
     cudaEvent_t fork, join[kAuxStreams];
+    int32_t *maxn_pin;                   // pinned copy of a call's multi-stripe maximum
+    cudaEvent_t maxn_ready;
 };
 
 // Per host thread and device: the auxiliary streams and fork/join events of
@@ -798,6 +800,8 @@ struct LaunchCfgs {
                 cudaEventDestroy(c->join[i]);
             }
             cudaEventDestroy(c->fork);
+            cudaEventDestroy(c->maxn_ready);
+            cudaFreeHost(c->maxn_pin);
             delete c;
         }
     }
@@ -835,6 +839,8 @@ static int launch_cfg(const LaunchCfg **out, int lane = 0) {
             TPZ_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
         }
         TPZ_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+        TPZ_CUDA(cudaEventCreateWithFlags(&c->maxn_ready, cudaEventDisableTiming));
+        TPZ_CUDA(cudaHostAlloc((void **)&c->maxn_pin, sizeof(int32_t), cudaHostAllocDefault));
         per_dev[dev] = c;
     }
     *out = per_dev[dev];
@@ -866,32 +872,38 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
     bin_scatter_kernel<<<std::max(gb, 1), 256, 0, st>>>(n, list, list_n, a.qlen, a.slen, cursor,
                                                         sorted, TPZ_SW_MAX_QLEN);
     launches += 4;
-    if (host_maxn) {
-        // the boundary buffer of multi-stripe bins is sized by the longest
-        // subject among queries longer than one stripe
-        if (known_maxn >= 0) {
-            *host_maxn = known_maxn;
-        } else {
-            TPZ_CUDA(cudaMemcpyAsync(host_maxn, multi_maxn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-            TPZ_CUDA(cudaStreamSynchronize(st));
-        }
-        if (*host_maxn > 0) {
-            a.bnd_words = 3 * ((int64_t)*host_maxn + 1);
-            const size_t bytes = sizeof(uint32_t) * (size_t)a.bnd_words * nsm *
-                                 cfg->blocks_per_sm[kMaxR - 1];
-            TPZ_CUDA(cudaMallocAsync((void **)&a.bnd, bytes, st));
+    // The boundary buffer of multi-stripe bins is sized by the longest subject
+    // among queries longer than one stripe.  When the caller does not know it,
+    // the device's count comes back while the single-stripe bins already run,
+    // and the multi-stripe bins are launched after them.
+    const bool defer = host_maxn && known_maxn < 0;
+    auto alloc_bnd = [&](int maxn, cudaStream_t s) -> int {
+        a.bnd_words = 3 * ((int64_t)maxn + 1);
+        const size_t bytes = sizeof(uint32_t) * (size_t)a.bnd_words * nsm *
+                             cfg->blocks_per_sm[kMaxR - 1];
+        TPZ_CUDA(cudaMallocAsync((void **)&a.bnd, bytes, s));
+        if (a16) { a16->bnd = a.bnd; a16->bnd_words = a.bnd_words; }
+        return TPZ_OK;
+    };
+    if (host_maxn && !defer) {
+        *host_maxn = known_maxn;
+        if (known_maxn > 0) {
+            const int rc = alloc_bnd(known_maxn, st);
+            if (rc) return rc;
         }
     }
-    if (a16) { a16->bnd = a.bnd; a16->bnd_words = a.bnd_words; }
+    if (defer) {
+        TPZ_CUDA(cudaMemcpyAsync(cfg->maxn_pin, multi_maxn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        TPZ_CUDA(cudaEventRecord(cfg->maxn_ready, st));
+    }
     // one persistent kernel per row bin, longest rows first, spread over the
     // auxiliary streams so that each kernel's tail overlaps the next one;
     // the multi-stripe bins share one boundary buffer and stay on aux[0]
     TPZ_CUDA(cudaEventRecord(cfg->fork, st));
     for (int i = 0; i < kAuxStreams; ++i) TPZ_CUDA(cudaStreamWaitEvent(cfg->aux[i], cfg->fork, 0));
     int rr = 0;
-    for (int b = kUsedRBins - 1; b >= 0; --b) {
+    auto launch_bin = [&](int b) {
         const int R = bin_rows(b), S = bin_stripes(b);
-        if (S > 1 && !a.bnd) continue;
         const int grid = nsm * cfg->blocks_per_sm[R - 1];
         cudaStream_t xs = S > 1 ? cfg->aux[0] : cfg->aux[rr++ % kAuxStreams];
         cfg->fn[R - 1]<<<grid, 32, cfg->smem[R - 1], xs>>>(a, b, S);
@@ -900,11 +912,29 @@ static int launch_round(const LaunchCfg *cfg, Args &a, int64_t n, const int32_t 
             cfg->fn[R - 1]<<<grid, 32, cfg->smem[R - 1], xs>>>(*a16, b, S);
             ++launches;
         }
+    };
+    for (int b = kUsedRBins - 1; b >= 0; --b) {
+        if (bin_stripes(b) > 1 && (defer || !a.bnd)) continue;
+        launch_bin(b);
     }
+    int rc = TPZ_OK;
+    if (defer) {
+        const cudaError_t e = cudaEventSynchronize(cfg->maxn_ready);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "multi-stripe maximum");
+        } else {
+            *host_maxn = *cfg->maxn_pin;
+            if (*host_maxn > 0 && (rc = alloc_bnd(*host_maxn, cfg->aux[0])) == TPZ_OK)
+                for (int b = kUsedRBins - 1; b >= kMaxR; --b) launch_bin(b);
+        }
+    }
+    // the join comes after every launch, also on an error above, so that the
+    // caller's stream waits for all kernels before it frees their buffers
     for (int i = 0; i < kAuxStreams; ++i) {
         TPZ_CUDA(cudaEventRecord(cfg->join[i], cfg->aux[i]));
         TPZ_CUDA(cudaStreamWaitEvent(st, cfg->join[i], 0));
     }
+    if (rc) return rc;
     TPZ_CUDA(cudaGetLastError());
     return TPZ_OK;
 }
@@ -1439,15 +1469,45 @@ int tpz_sw_batch_host(int64_t n, const int8_t *q, const int64_t *qoff, const int
         cut[1] = n / 16; cut[2] = 4 * (n / 16); cut[3] = n;
         nch = 3;
     }
-    // host-side validation and the byte ranges each chunk reads, chunks
-    // scanned on their own threads
+    // host-side validation and the byte ranges each chunk reads: the chunks
+    // cut into pieces in proportion to their size, scanned on up to 16 host
+    // threads, and merged per chunk
     Span sp[kMaxChunks];
     {
+        const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        struct Piece { int c; int64_t i0, i1; Span r; };
+        std::vector<Piece> pieces;
+        for (int c = 0; c < nch; ++c) {
+            const int64_t m = cut[c + 1] - cut[c];
+            // at least 32,768 pairs per piece: a thread costs more than that
+            const int64_t k = std::max<int64_t>(1, std::min((nt * m + n - 1) / n, m / 32768));
+            for (int64_t p = 0; p < k; ++p)
+                pieces.push_back({c, cut[c] + m * p / k, cut[c] + m * (p + 1) / k, Span{}});
+        }
         std::vector<std::thread> th;
-        for (int c = 1; c < nch; ++c)
-            th.emplace_back([&, c]() { sp[c] = scan_pairs(cut[c], cut[c + 1], qoff, qlen, soff, slen); });
-        sp[0] = scan_pairs(cut[0], cut[1], qoff, qlen, soff, slen);
+        for (size_t p = 1; p < pieces.size(); ++p)
+            th.emplace_back([&, p]() {
+                pieces[p].r = scan_pairs(pieces[p].i0, pieces[p].i1, qoff, qlen, soff, slen);
+            });
+        pieces[0].r = scan_pairs(pieces[0].i0, pieces[0].i1, qoff, qlen, soff, slen);
         for (auto &t : th) t.join();
+        for (int c = 0; c < nch; ++c) sp[c] = Span{INT64_MAX, 0, INT64_MAX, 0, -1, 0};
+        for (const Piece &p : pieces) {
+            Span &d = sp[p.c];
+            const Span &r = p.r;
+            if (r.bad >= 0 && (d.bad < 0 || r.bad < d.bad)) d.bad = r.bad;
+            d.multi_maxn = std::max(d.multi_maxn, r.multi_maxn);
+            if (p.i1 > p.i0) {
+                d.qlo = std::min(d.qlo, r.qlo);
+                d.qhi = std::max(d.qhi, r.qhi);
+                if (r.shi > r.slo || r.shi > 0) {
+                    d.slo = std::min(d.slo, r.slo);
+                    d.shi = std::max(d.shi, r.shi);
+                }
+            }
+        }
+        for (int c = 0; c < nch; ++c)
+            if (sp[c].slo > sp[c].shi) sp[c].slo = sp[c].shi;
     }
     int64_t qbytes = 0, sbytes = 0;
     for (int c = 0; c < nch; ++c) {
