@@ -56,3 +56,20 @@ def test_sw_rejects_bad_gaps_and_sizes_before_device_work():
     with pytest.raises(native.TopazError) as e:
         native.sw_batch_host(np.zeros(9000, np.int8), [0], [9000], q, [0], [4], synth.matrix())
     assert e.value.code == -4                         # qlen above the limit
+
+
+def test_sw_host_names_the_first_bad_pair_of_a_large_batch():
+    # a batch the host entry point cuts into chunks and scans in pieces on
+    # several threads: the error names the first invalid pair, whichever
+    # piece finds it first
+    n = 300_000
+    q = np.zeros(64, np.int8)
+    qlen = np.full(n, 8, np.int32)
+    qlen[250_001] = 0
+    qlen[70_123] = 9000
+    qlen[140_000] = -1
+    with pytest.raises(native.TopazError) as e:
+        native.sw_batch_host(q, np.zeros(n, np.int64), qlen, q, np.zeros(n, np.int64),
+                             np.full(n, 8, np.int32), synth.matrix())
+    assert e.value.code == -4
+    assert "pair 70123 " in str(e.value)
