@@ -154,7 +154,7 @@ __device__ __forceinline__ uint32_t letter_pair(const Args &a, const int8_t *sA,
 // qm_rerun / qm_rerun_count when given, else to a.rerun / a.rerun_count.
 // QM = true also means that profA/profB already hold the query profile
 // (both pairs share it).
-template <int R, bool MULTI, bool QM = false>
+template <int R, bool MULTI, bool QM = false, bool SCORE = false>
 __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const int8_t *smat,
                                          uint32_t *profA, uint32_t *profB, uint16_t *ring,
                                          int stripes, uint32_t *bnd, int qm_lanes = 0,
@@ -341,7 +341,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             Xa[r] = __viaddmax_s16x2_relu(r == 0 ? D : H[r - 1], sc, E[r]);
             Xga[r] = __viaddmax_s16x2(Xa[r], NGO, NEGINF);
         }
-        search();
+        if constexpr (!SCORE) search();
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const uint32_t Hn = __vimax_s16x2_relu(Xa[r], F);
@@ -370,10 +370,12 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             uint32_t *b = bnd + 3 * (size_t)j;
             b[0] = outH; b[1] = outF; b[2] = outFm;
         }
-        pend = cm != thr;
-        pcm = cm;
-        pthr = thr;
-        pj = j;
+        if constexpr (!SCORE) {
+            pend = cm != thr;
+            pcm = cm;
+            pthr = thr;
+            pj = j;
+        }
         runmax = cm;
         diag = inH;
     };
@@ -411,7 +413,7 @@ __device__ __forceinline__ void run_task(const Args &a, int pA, int pB, const in
             step(k + 1, wa2, wb2, wa, wb);
         }
     }
-    search();                           // the last column's, if it rose
+    if constexpr (!SCORE) search();     // the last column's, if it rose
 
     if (a.score_only || decided) { colA = colB = 0; rowA = rowB = 0; }
     kA = max(kA, best_key(lo16(runmax), colA, rowA));
@@ -585,7 +587,9 @@ __device__ __forceinline__ void qm_build_profile(const Args &a, int64_t p, const
     }
 }
 
-template <int R>
+// SCORE: scores only (report-mode search), with the end-coordinate row
+// search compiled out rather than skipped at run time
+template <int R, bool SCORE>
 __global__ void __launch_bounds__(kQmWarps * 32) sw_query_kernel(const __grid_constant__ Args a,
                                                                  QmArgs g, int bin) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -642,7 +646,7 @@ __global__ void __launch_bounds__(kQmWarps * 32) sw_query_kernel(const __grid_co
             if (2 * t >= n) break;
             const int pA = (int)(uint32_t)keys[2 * t];
             const int pB = 2 * t + 1 < n ? (int)(uint32_t)keys[2 * t + 1] : -1;
-            run_task<R, false, true>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 16, sat,
+            run_task<R, false, true, SCORE>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 16, sat,
                                      &s_nsat);
         }
         __syncthreads();
@@ -657,7 +661,7 @@ __global__ void __launch_bounds__(kQmWarps * 32) sw_query_kernel(const __grid_co
             if (2 * t >= ns) break;
             const int pA = sat[2 * t];
             const int pB = 2 * t + 1 < ns ? sat[2 * t + 1] : -1;
-            run_task<R, false, true>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 8, nullptr,
+            run_task<R, false, true, SCORE>(a, pA, pB, smat, prof, prof, ring, 1, nullptr, 8, nullptr,
                                      nullptr);
         }
     }
@@ -1105,22 +1109,23 @@ int batch_device_x(int64_t n, const int8_t *q, const int64_t *qoff, const int32_
 // kernels of the same call.
 struct QmCfg {
     typedef void (*Fn)(const Args, QmArgs, int);
-    Fn fn[kMaxR];
-    int blocks_per_sm[kMaxR];
+    Fn fn[2][kMaxR];                    // [score only][R - 1]
+    int blocks_per_sm[2][kMaxR];
     cudaStream_t aux[kQmStreams];
     cudaEvent_t fork, join[kQmStreams];
 };
 
 template <int R>
 struct QmTable {
-    static void fill(QmCfg::Fn *k) {
-        k[R - 1] = sw_query_kernel<R>;
+    static void fill(QmCfg::Fn (*k)[kMaxR]) {
+        k[0][R - 1] = sw_query_kernel<R, false>;
+        k[1][R - 1] = sw_query_kernel<R, true>;
         QmTable<R - 1>::fill(k);
     }
 };
 template <>
 struct QmTable<0> {
-    static void fill(QmCfg::Fn *) {}
+    static void fill(QmCfg::Fn (*)[kMaxR]) {}
 };
 
 struct QmCfgs {
@@ -1143,18 +1148,18 @@ static int qm_cfg(const QmCfg **out) {
     if (!cfgs.per_dev[dev]) {
         QmCfg *c = new QmCfg();
         QmTable<kMaxR>::fill(c->fn);
-        for (int r = 1; r <= kMaxR; ++r) {
-            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          qm_smem_bytes(r)));
-            TPZ_CUDA(cudaFuncSetAttribute((const void *)c->fn[r - 1],
-                                          cudaFuncAttributePreferredSharedMemoryCarveout,
-                                          (int)cudaSharedmemCarveoutMaxShared));
-            int nb = 0;
-            TPZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)c->fn[r - 1],
-                                                                   kQmWarps * 32, qm_smem_bytes(r)));
-            c->blocks_per_sm[r - 1] = std::max(1, nb);
-        }
+        for (int so = 0; so < 2; ++so)
+            for (int r = 1; r <= kMaxR; ++r) {
+                const void *f = (const void *)c->fn[so][r - 1];
+                TPZ_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              qm_smem_bytes(r)));
+                TPZ_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                              (int)cudaSharedmemCarveoutMaxShared));
+                int nb = 0;
+                TPZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, kQmWarps * 32,
+                                                                       qm_smem_bytes(r)));
+                c->blocks_per_sm[so][r - 1] = std::max(1, nb);
+            }
         for (int i = 0; i < kQmStreams; ++i) {
             TPZ_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
             TPZ_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
@@ -1264,10 +1269,11 @@ int batch_device_grouped(int64_t n, const int8_t *q, const int64_t *qoff, const 
         for (int r = 1; r <= kMaxR; ++r) if (!per_r[r - 1].empty()) order.push_back(r);
         std::sort(order.begin(), order.end(), [&](int x, int y) { return work[x - 1] > work[y - 1]; });
         int k = 0;
+        const int so = a.score_only ? 1 : 0;
         for (int r : order) {
-            const int grid = (int)std::min<int64_t>((int64_t)nsm * qc->blocks_per_sm[r - 1],
+            const int grid = (int)std::min<int64_t>((int64_t)nsm * qc->blocks_per_sm[so][r - 1],
                                                     (int64_t)per_r[r - 1].size() / 2);
-            qc->fn[r - 1]<<<grid, kQmWarps * 32, qm_smem_bytes(r), qc->aux[k++ % kQmStreams]>>>(
+            qc->fn[so][r - 1]<<<grid, kQmWarps * 32, qm_smem_bytes(r), qc->aux[k++ % kQmStreams]>>>(
                 a, g, r - 1);
             ++launches;
         }
