@@ -839,7 +839,8 @@ def native_arm(args, rank, local_rank, world):
         torch.cuda.empty_cache()
         large = large_bench(args, dev)
     if rank == 0:
-        cpu = None if args.no_cpu_baseline else cpu_baseline_sw(ps, mat)
+        # the host-core baseline is an N=1 figure: rank 0 of a single-GPU run
+        cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline_sw(ps, mat)
         traffic_per_cell = read_traffic()
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world,
