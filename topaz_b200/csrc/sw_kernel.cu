@@ -43,9 +43,16 @@
 // Pairs are binned on the device by R = ceil(qlen/32) and by subject length
 // (counting sort), paired two per task within a bin, and drained by one
 // persistent kernel per R from an atomic task counter.  Pairs whose u8-pass
-// maximum saturates are appended to a rerun list and re-run with the i16
-// lane length (seg = ceil(qlen/8)).  With qlen <= 1024 and |M| <= 127 no
-// score can reach 32767, so 16-bit arithmetic is exact.
+// maximum saturates are appended to their bin's rerun list and re-run with
+// the i16 lane length (seg = ceil(qlen/8)) by a second kernel of the bin on
+// the same stream.  With qlen <= 1024 and |M| <= 127 no score can reach
+// 32767, so 16-bit arithmetic is exact.
+//
+// Every lane computes every step, also before its first column and past
+// the subject's end (pad letters there), so the step body has no per-lane
+// column test; the refresh every 32 steps and the row search of a risen
+// column (one step late, between the next column's two phases) are the
+// only branches.
 
 #include <stdio.h>
 #include <string.h>
