@@ -86,6 +86,35 @@ def test_sw_every_row_bin_and_odd_batch(cuda):
     assert (got == ref).all()
 
 
+
+def test_sw_short_subjects_and_wavefront_edges(cuda):
+    # every lane computes every step, before its first column and past the
+    # subject's end: subjects of 0-2 columns, around the 32-column wavefront
+    # fill and the 32-step refresh, next to queries on and around the
+    # stripe and lane-segment boundaries; random, self and strongly
+    # homologous content (the latter saturates the u8 pass), in one batch so
+    # short and long subjects share bins and tasks
+    rng = np.random.default_rng(31)
+    qs, ss = [], []
+    for ql in (1, 2, 31, 32, 33, 96, 352, 1000, 1024, 1025):
+        q = rng.integers(0, 20, ql).astype(np.int8)
+        for sl in (0, 1, 2, 31, 32, 33, 63, 64, 65, 97, 500):
+            qs.append(q); ss.append(rng.integers(0, 20, sl).astype(np.int8))
+            qs.append(q); ss.append(np.resize(q, sl).astype(np.int8))
+    ql = np.array([len(x) for x in qs], np.int32); sl = np.array([len(x) for x in ss], np.int32)
+    qo = np.concatenate([[0], np.cumsum(ql)[:-1]]).astype(np.int64)
+    so = np.concatenate([[0], np.cumsum(sl)[:-1]]).astype(np.int64)
+    s_all = np.concatenate(ss) if sl.sum() else np.zeros(0, np.int8)
+    ps = synth.PairSet(np.concatenate(qs), qo, ql, s_all, so, sl, 0)
+    mat = synth.matrix("BLOSUM62")
+    got = _run_dev(cuda, ps, mat)
+    ref = np.stack(oracle.oracle_sw(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat))
+    bad = np.flatnonzero((got != ref).any(axis=0))
+    assert bad.size == 0, (bad[:5], got[:, bad[:5]], ref[:, bad[:5]], ps.qlen[bad[:5]], ps.slen[bad[:5]])
+    assert (ref[0] + 4 >= 255).any()                 # some pairs took the i16 pass
+    host = np.stack(native.sw_batch_host(ps.q, ps.qoff, ps.qlen, ps.s, ps.soff, ps.slen, mat))
+    assert (host == ref).all()
+
 def test_sw_full_size_sample_and_order_independence(cuda):
     ps = synth.sw_pairs(1_000_000, seed=1)
     mat = synth.matrix("BLOSUM62")
