@@ -94,48 +94,57 @@ __global__ void text_check_kernel(const uint8_t *T, int64_t Tsize, int *bad) {
 }
 
 // Host -> device copy of pageable memory (the .psq and .SA file mappings):
-// host threads copy 64 MB pieces into two pinned buffers in turn -- touching
+// host threads copy 32 MB pieces into two pinned buffers in turn -- touching
 // the mapping's pages in parallel -- while the previous piece is on its way
-// to the device.
-int upload_pageable(void *dst, const void *src, size_t n) {
-    constexpr size_t kPiece = 64ull << 20;
-    if (n <= kPiece)
-        return cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice) == cudaSuccess
-                   ? TPZ_OK : tpz::cuda_fail(cudaGetLastError(), "index upload");
-    cudaStream_t st = cudaStreamPerThread;
+// to the device.  The pinned buffers are made once per index and serve both
+// files (pinning memory costs about as much as copying it).
+struct UploadStage {
+    static constexpr size_t kPiece = 32ull << 20;
     uint8_t *pin[2] = {nullptr, nullptr};
     cudaEvent_t done[2] = {nullptr, nullptr};
+    int init() {
+        for (int b = 0; b < 2; ++b)
+            if (cudaHostAlloc((void **)&pin[b], kPiece, cudaHostAllocDefault) != cudaSuccess ||
+                cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) != cudaSuccess)
+                return tpz::cuda_fail(cudaGetLastError(), "index upload buffers");
+        return TPZ_OK;
+    }
+    ~UploadStage() {
+        for (int b = 0; b < 2; ++b) {
+            if (done[b]) cudaEventDestroy(done[b]);
+            if (pin[b]) cudaFreeHost(pin[b]);
+        }
+    }
+};
+
+int upload_pageable(UploadStage &stg, void *dst, const void *src, size_t n) {
+    constexpr size_t kPiece = UploadStage::kPiece;
+    cudaStream_t st = cudaStreamPerThread;
     int rc = TPZ_OK;
-    for (int b = 0; b < 2 && rc == TPZ_OK; ++b)
-        if (cudaHostAlloc((void **)&pin[b], kPiece, cudaHostAllocDefault) != cudaSuccess ||
-            cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) != cudaSuccess)
-            rc = tpz::cuda_fail(cudaGetLastError(), "index upload buffers");
     const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     const uint8_t *s8 = (const uint8_t *)src;
     for (size_t off = 0, k = 0; rc == TPZ_OK && off < n; off += kPiece, ++k) {
         const size_t len = std::min(kPiece, n - off);
-        uint8_t *buf = pin[k & 1];
-        if (k >= 2 && cudaEventSynchronize(done[k & 1]) != cudaSuccess) {
+        uint8_t *buf = stg.pin[k & 1];
+        // the buffer's previous piece (of this or the other file) has left
+        if (cudaEventSynchronize(stg.done[k & 1]) != cudaSuccess) {
             rc = tpz::cuda_fail(cudaGetLastError(), "index upload");
             break;
         }
         const size_t part = (len + nt - 1) / nt;
         std::vector<std::thread> th;
-        for (unsigned t = 0; t < nt && (size_t)t * part < len; ++t) {
+        for (unsigned t = 1; t < nt && (size_t)t * part < len; ++t) {
             const size_t a = (size_t)t * part, e = std::min(len, a + part);
             th.emplace_back([=] { memcpy(buf + a, s8 + off + a, e - a); });
         }
+        memcpy(buf, s8 + off, std::min(len, part));
         for (std::thread &x : th) x.join();
         if (cudaMemcpyAsync((uint8_t *)dst + off, buf, len, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            cudaEventRecord(done[k & 1], st) != cudaSuccess)
+            cudaEventRecord(stg.done[k & 1], st) != cudaSuccess)
             rc = tpz::cuda_fail(cudaGetLastError(), "index upload");
     }
     if (cudaStreamSynchronize(st) != cudaSuccess && rc == TPZ_OK)
         rc = tpz::cuda_fail(cudaGetLastError(), "index upload");
-    for (int b = 0; b < 2; ++b) {
-        if (done[b]) cudaEventDestroy(done[b]);
-        if (pin[b]) cudaFreeHost(pin[b]);
-    }
     return rc;
 }
 
@@ -644,8 +653,12 @@ int tpz_index_create(const uint8_t *T, int64_t Tsize, const int64_t *SA, const v
         cudaMemset(dSA + Tsize, 0, (sa_rows - Tsize) * 8) != cudaSuccess ||
         cudaMemcpy(dps, pstart.data(), (Psize + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(tpz::cuda_fail(cudaGetLastError(), "tpz_index_create copies"));
-    if ((rc = upload_pageable(dT, T, Tsize)) || (rc = upload_pageable(dSA, SA, Tsize * 8)))
-        return fail(rc);
+    {
+        UploadStage stg;
+        if ((rc = stg.init()) || (rc = upload_pageable(stg, dT, T, Tsize)) ||
+            (rc = upload_pageable(stg, dSA, SA, Tsize * 8)))
+            return fail(rc);
+    }
     int *dbad;
     if ((rc = dalloc(ix, (void **)&dbad, 4))) return fail(rc);
     cudaMemset(dbad, 0, 4);
